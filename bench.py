@@ -1,0 +1,304 @@
+"""HEOM propagation benchmark: ADO-steps/s of the fused FP64 propagator.
+
+Workload (default): transverse-field Ising spin glass, N=6 spins (d=64),
+J_ij ~ N(0,1) (seeded splitmix64/Box-Muller), h=1, one Drude-Lorentz bath
+per spin (lambda=0.1, gamma=1, T=1), Pade K=2 (18 modes), depth L=4
+(max_depth 5) -> 7315 ADOs of 64x64 complex128 (0.479 GB per state),
+RK4 (4-term Taylor, Horner form), dt=0.005.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N>1).  A single hierarchy does not shard:
+N>1 runs N independent replicas (seed + rank), value = total ADO-steps/s.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from helix_b200 import systems as S  # noqa: E402
+
+METRIC = "ADO-steps/s on 1 B200, chosen form vs plain FP64, at rho0 trace-dist <=1e-6"
+UNIT = "ADO-steps/s"
+
+CONFIGS = {
+    "c2": dict(n=6, depth=4, K=2, h=1.0, dt=0.005, seed=2025,
+               workload="spin_glass_d64_L4_K2_7315ados_fp64"),
+    "c1": dict(n=4, depth=3, K=2, h=1.0, dt=0.01, seed=2024,
+               workload="spin_glass_d16_L3_K2_455ados_fp64"),
+}
+
+
+def make_problem(cfg: dict, rank: int = 0):
+    return S.spin_glass(cfg["n"], seed=cfg["seed"] + rank, depth=cfg["depth"], K=cfg["K"], h=cfg["h"],
+                        dt=cfg["dt"])
+
+
+def load_peaks() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(config: str) -> float | None:
+    """DRAM bytes per stage launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"stage_kernel_{config}_ncu.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(cfg: dict, steps: int) -> dict:
+    """Time the FP64 CPU oracle (the reference has no CPU path) on host cores."""
+    from oracle import oracle as O
+    p = make_problem(cfg)
+    o = O.Oracle(p)
+    o.run(1)  # warm
+    t0 = time.perf_counter()
+    o.run(steps)
+    dt = time.perf_counter() - t0
+    size = o.size
+    o.close()
+    return {"value": size * steps / dt, "unit": UNIT, "cores": O.threads(), "kind": "port",
+            "sample": f"{steps} full steps of the {size}-ADO hierarchy ({cfg['workload']}), FP64 oracle, OpenMP"}
+
+
+def run_reference(args, cfg: dict) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    p = make_problem(cfg)
+    o = O.Oracle(p)
+    for _ in range(args.warmup):
+        o.run(1)
+    t0 = time.perf_counter()
+    o.run(args.steps)
+    sec = time.perf_counter() - t0
+    value = o.size * args.steps / sec
+    threads = O.threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "ados": o.size, "dim": p.dim, "modes": p.modes,
+                   "dt": p.dt, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full steps of the {o.size}-ADO hierarchy; the reference has no "
+                                   "CPU path, so its FP64 restatement (oracle/heom_oracle.cpp) stands in"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    o.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, cfg: dict) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from helix_b200 import capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    p = make_problem(cfg, rank)
+    ctx = capi.Context(p)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    H = ctx.size
+    state_bytes = int(ctx.info.state_bytes)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident throughput (value) --------------------------------
+    for _ in range(args.warmup):
+        ctx.step(1)
+    ctx.sync()
+    c0 = ctx.counters()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ctx.step(args.steps)
+    ev1.record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    c1 = ctx.counters()
+    launches = int(c1.kernel_launches - c0.kernel_launches)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    barrier()
+    value = world * H * args.steps / (ms / 1000.0)
+
+    # roofline of the stage kernel: Horner form moves 11 state volumes per step
+    # (stage 1: read rho, write u1; stages 2-4: read u, read rho, write)
+    stages = int(ctx.info.kernels_per_step)
+    alg_bytes_per_step = (3 * stages - 1) * state_bytes
+    per_launch_bytes = alg_bytes_per_step / stages
+    launch_ms = ms / (args.steps * stages)
+    achieved = per_launch_bytes / (launch_ms / 1000.0) / 1e9
+    peak, peak_kind = load_peaks()
+    traffic = profiled_traffic(args.config)
+
+    # ---- end to end through the C ABI with host buffers (e2e) --------------
+    pinned = torch.empty(H * p.dim * p.dim * 2, dtype=torch.float64, pin_memory=True)
+    host_state = pinned.numpy().view(np.complex128).reshape(H, p.dim, p.dim)
+    host_state[:] = 0
+    host_state[0] = S.initial_rho0(p.dim)
+    rho_trace = torch.empty(args.steps * p.dim * p.dim * 2, dtype=torch.float64, pin_memory=True).numpy()
+    en_trace = np.zeros(args.steps)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.set_state(host_state)
+    ctx.step_trace_into(args.steps, rho_trace, en_trace)
+    final = ctx.rho0()
+    e2e_sec = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_sec], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_sec = float(t.item())
+    e2e_value = world * H * args.steps / e2e_sec
+    assert np.isfinite(final).all() and np.isfinite(en_trace).all()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cfg, args.cpu_steps)
+
+    ctx.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "ados": H, "dim": p.dim, "modes": p.modes, "depth_L": cfg["depth"],
+                       "dt": p.dt, "integrator": "RK4 (4-term Taylor, Horner form)",
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": f"inputs larger than L2 (state {state_bytes / 1e9:.3f} GB)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                         else "fallback 6650 GB/s",
+                         "algorithmic_bytes_per_launch": per_launch_bytes,
+                         "kernel": "stage_kernel<6>", "launch_ms": launch_ms},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
+                    "d2h_bytes_per_step": p.dim * p.dim * 16 + 24,
+                    "path": "hx_ctx_write_state (pinned host) + hx_ctx_step_trace (rho0, <H> per step) + hx_ctx_read_rho0"},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

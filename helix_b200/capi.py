@@ -1,0 +1,277 @@
+"""ctypes binding of the helix_b200 C ABI (include/helix_b200.h).
+
+The CUDA library must exist in-tree (``helix_b200/_build/libhelix_b200.so``,
+built by ``helix_b200/build.py``); there is no fallback path: a missing
+library or a failed call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+from . import build as _build
+
+HX_OK = 0
+STATUS_NAMES = {
+    1: "InvalidDimension", 2: "InvalidRowOffsets", 3: "InvalidColumnValueSize", 4: "InvalidColumnIndex",
+    5: "InvalidCouplingDimension", 6: "InvalidRuntimeOption", 7: "UnsupportedPrecision",
+    8: "UnsupportedBackend", 9: "UnsupportedSystemKind", 10: "UnsupportedExecution",
+    11: "UnsupportedBath", 12: "UnsupportedHierarchy", 13: "ConcurrentContextUnsupported",
+    14: "BathExponentsInvalid", 15: "CudaFailure", 16: "OutOfMemory", 17: "NonFiniteState",
+    18: "DeviceWaitTimeout",
+}
+PRECISION_DOUBLE = 1
+
+# Every exported symbol of include/helix_b200.h
+EXPORTS = [
+    "hx_last_error", "hx_version", "hx_hierarchy_size", "hx_hierarchy_tables", "hx_psd",
+    "hx_seeded_couplings", "hx_ctx_create", "hx_ctx_destroy", "hx_ctx_set_stream", "hx_ctx_get_stream",
+    "hx_ctx_info", "hx_ctx_counters", "hx_ctx_step", "hx_ctx_step_trace", "hx_ctx_sync",
+    "hx_ctx_read_rho0", "hx_ctx_observables", "hx_ctx_read_state", "hx_ctx_write_state",
+    "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_check_finite",
+]
+
+
+class HxError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        self.code = code
+        self.status = STATUS_NAMES.get(code, f"code{code}")
+        super().__init__(f"{self.status}: {message}")
+
+
+class _Bath(C.Structure):
+    _fields_ = [("inverse_temperature", C.c_double), ("damping", C.c_double),
+                ("coupling_strength", C.c_double), ("pade_terms", C.c_uint32),
+                ("coupling_diag", C.POINTER(C.c_double))]
+
+
+class _Problem(C.Structure):
+    _fields_ = [("dim", C.c_uint32), ("h_diag", C.POINTER(C.c_double)), ("h_flip", C.POINTER(C.c_double)),
+                ("n_baths", C.c_uint32), ("baths", C.POINTER(_Bath)), ("max_depth", C.c_uint32),
+                ("time_step", C.c_double), ("integration_order", C.c_uint32), ("precision", C.c_uint32),
+                ("flags", C.c_uint32)]
+
+
+class Info(C.Structure):
+    _fields_ = [("dim", C.c_uint32), ("modes", C.c_uint32), ("hierarchy_size", C.c_uint64),
+                ("state_bytes", C.c_uint64), ("device_bytes", C.c_uint64), ("steps_done", C.c_uint64),
+                ("time", C.c_double), ("kernels_per_step", C.c_uint32)]
+
+
+class Counters(C.Structure):
+    _fields_ = [("kernel_launches", C.c_uint64), ("stage_launches", C.c_uint64),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def lib():
+    """Load the in-tree CUDA library (raises if it was not built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            path = library_path()
+            if not os.path.exists(path):
+                raise FileNotFoundError(
+                    f"{path} is missing: build it with `python -m helix_b200.build` (no CPU fallback exists)")
+            L = C.CDLL(path)
+            vp, u32, u64, dp = C.c_void_p, C.c_uint32, C.c_uint64, C.POINTER(C.c_double)
+            L.hx_last_error.restype = C.c_char_p
+            L.hx_version.restype = C.c_char_p
+            L.hx_hierarchy_size.argtypes = [u32, u32, C.POINTER(u64)]
+            L.hx_hierarchy_tables.argtypes = [u32, u32, vp, vp, u64]
+            L.hx_psd.argtypes = [u32, vp, vp]
+            L.hx_seeded_couplings.argtypes = [u32, u64, vp]
+            L.hx_ctx_create.argtypes = [C.POINTER(_Problem), C.POINTER(vp)]
+            L.hx_ctx_destroy.argtypes = [vp]
+            L.hx_ctx_destroy.restype = None
+            L.hx_ctx_set_stream.argtypes = [vp, vp]
+            L.hx_ctx_get_stream.argtypes = [vp, C.POINTER(vp)]
+            L.hx_ctx_info.argtypes = [vp, C.POINTER(Info)]
+            L.hx_ctx_counters.argtypes = [vp, C.POINTER(Counters)]
+            L.hx_ctx_step.argtypes = [vp, u64]
+            L.hx_ctx_step_trace.argtypes = [vp, u64, vp, vp]
+            L.hx_ctx_sync.argtypes = [vp]
+            L.hx_ctx_read_rho0.argtypes = [vp, vp, u64]
+            L.hx_ctx_observables.argtypes = [vp, dp, dp, dp]
+            L.hx_ctx_read_state.argtypes = [vp, vp, u64]
+            L.hx_ctx_write_state.argtypes = [vp, vp, u64]
+            L.hx_ctx_state_device_ptr.argtypes = [vp, C.POINTER(vp)]
+            L.hx_ctx_rhs.argtypes = [vp, vp, u64]
+            L.hx_ctx_check_finite.argtypes = [vp]
+            _lib = L
+        return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != HX_OK:
+        raise HxError(rc, lib().hx_last_error().decode())
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def version() -> str:
+    return lib().hx_version().decode()
+
+
+def hierarchy_size(modes: int, max_depth: int) -> int:
+    out = C.c_uint64(0)
+    _check(lib().hx_hierarchy_size(modes, max_depth, C.byref(out)))
+    return int(out.value)
+
+
+def hierarchy_tables(modes: int, max_depth: int):
+    """(rows[H, M], edges[H, 2M]) built on the device, reference order and sentinel."""
+    H = hierarchy_size(modes, max_depth)
+    rows = np.zeros((H, modes), np.int32)
+    edges = np.zeros((H, 2 * modes), np.int32)
+    _check(lib().hx_hierarchy_tables(modes, max_depth, _p(rows), _p(edges), H))
+    return rows, edges
+
+
+def psd(K: int):
+    p = np.zeros(max(K, 1))
+    r = np.zeros(max(K, 1))
+    _check(lib().hx_psd(K, _p(p), _p(r)))
+    return p[:K], r[:K]
+
+
+def seeded_couplings(n: int, seed: int) -> np.ndarray:
+    J = np.zeros((n, n))
+    _check(lib().hx_seeded_couplings(n, seed, _p(J)))
+    return J
+
+
+class Context:
+    """One HEOM problem resident on the current CUDA device (wraps hx_ctx)."""
+
+    def __init__(self, problem, order: int = 4, dt: float | None = None):
+        L = lib()
+        self.problem = problem
+        d = problem.dim
+        self._keep = []
+        hd = np.ascontiguousarray(problem.h_diag, np.float64)
+        hf = np.ascontiguousarray(problem.h_flip, np.float64)
+        self._keep += [hd, hf]
+        baths = (_Bath * len(problem.baths))()
+        for j, b in enumerate(problem.baths):
+            if b.v_diag is None:
+                raise HxError(11, "the fused path needs diagonal coupling operators")
+            v = np.ascontiguousarray(b.v_diag, np.float64)
+            if v.ndim != 1 or v.shape[0] < d:
+                raise HxError(5, "coupling operator dimensions must match the system operator")
+            self._keep.append(v)
+            baths[j] = _Bath(b.beta, b.gamma, b.zeta, b.K, v.ctypes.data_as(C.POINTER(C.c_double)))
+        self._keep.append(baths)
+        prob = _Problem(d, hd.ctypes.data_as(C.POINTER(C.c_double)), hf.ctypes.data_as(C.POINTER(C.c_double)),
+                        len(problem.baths), baths, problem.max_depth,
+                        problem.dt if dt is None else dt, order, PRECISION_DOUBLE, 0)
+        h = C.c_void_p()
+        _check(L.hx_ctx_create(C.byref(prob), C.byref(h)))
+        self._h = h
+        self.info = self.get_info()
+        self.size = int(self.info.hierarchy_size)
+        self.dim = d
+
+    # lifecycle -----------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().hx_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # queries -------------------------------------------------------------
+    def get_info(self) -> Info:
+        info = Info()
+        _check(lib().hx_ctx_info(self._h, C.byref(info)))
+        return info
+
+    def counters(self) -> Counters:
+        c = Counters()
+        _check(lib().hx_ctx_counters(self._h, C.byref(c)))
+        return c
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        _check(lib().hx_ctx_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().hx_ctx_get_stream(self._h, C.byref(s)))
+        return int(s.value or 0)
+
+    def state_device_ptr(self) -> int:
+        p = C.c_void_p()
+        _check(lib().hx_ctx_state_device_ptr(self._h, C.byref(p)))
+        return int(p.value)
+
+    # propagation ---------------------------------------------------------
+    def step(self, nsteps: int = 1) -> None:
+        _check(lib().hx_ctx_step(self._h, nsteps))
+
+    def sync(self) -> None:
+        _check(lib().hx_ctx_sync(self._h))
+
+    def step_trace(self, nsteps: int, rho0: bool = True, energy: bool = True):
+        d = self.dim
+        r = np.zeros((nsteps, d, d), np.complex128) if rho0 else None
+        e = np.zeros(nsteps) if energy else None
+        _check(lib().hx_ctx_step_trace(self._h, nsteps, _p(r) if rho0 else None, _p(e) if energy else None))
+        return r, e
+
+    def step_trace_into(self, nsteps: int, rho0_buf: np.ndarray | None, energy_buf: np.ndarray | None) -> None:
+        _check(lib().hx_ctx_step_trace(self._h, nsteps, None if rho0_buf is None else _p(rho0_buf),
+                                       None if energy_buf is None else _p(energy_buf)))
+
+    # results -------------------------------------------------------------
+    def rho0(self) -> np.ndarray:
+        out = np.zeros((self.dim, self.dim), np.complex128)
+        _check(lib().hx_ctx_read_rho0(self._h, _p(out), 2 * out.size))
+        return out
+
+    def observables(self):
+        e, tr, ti = C.c_double(), C.c_double(), C.c_double()
+        _check(lib().hx_ctx_observables(self._h, C.byref(e), C.byref(tr), C.byref(ti)))
+        return e.value, complex(tr.value, ti.value)
+
+    def state(self) -> np.ndarray:
+        out = np.zeros((self.size, self.dim, self.dim), np.complex128)
+        _check(lib().hx_ctx_read_state(self._h, _p(out), 2 * out.size))
+        return out
+
+    def read_state_into(self, out: np.ndarray) -> None:
+        _check(lib().hx_ctx_read_state(self._h, _p(out), 2 * out.size))
+
+    def set_state(self, s: np.ndarray) -> None:
+        s = np.ascontiguousarray(s, np.complex128)
+        assert s.size == self.size * self.dim * self.dim
+        _check(lib().hx_ctx_write_state(self._h, _p(s), 2 * s.size))
+
+    def rhs(self) -> np.ndarray:
+        out = np.zeros((self.size, self.dim, self.dim), np.complex128)
+        _check(lib().hx_ctx_rhs(self._h, _p(out), 2 * out.size))
+        return out
+
+    def check_finite(self) -> None:
+        _check(lib().hx_ctx_check_finite(self._h))

@@ -1,0 +1,500 @@
+// Context lifecycle and the C ABI entry points of helix_b200 that touch the
+// device.  One context = one HEOM problem resident on one GPU: hierarchy
+// tables, per-ADO weights, operator diagonals and three state buffers
+// (rho and two stage buffers; the Horner form needs no separate sum buffer).
+//
+// Replaces the reference's process-global device state (src/matrix_storage.cu:4-23),
+// its session lifecycle (src/library/legacy_runtime_session.cu:53-118) and
+// develop() (src/liouville.cu:502-590).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "hx_internal.h"
+
+using hx::fail;
+
+namespace {
+
+template <typename T>
+int dev_alloc(hx_ctx* c, T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    const size_t bytes = count * sizeof(T);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    if (e != cudaSuccess) return hx::cuda_fail(e, "cudaMalloc");
+    c->device_bytes += bytes;
+    return HX_OK;
+}
+
+template <typename T>
+int upload(hx_ctx* c, T* dst, const std::vector<T>& src)
+{
+    if (src.empty()) return HX_OK;
+    HX_CUDA_TRY(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    c->counters.h2d_bytes += src.size() * sizeof(T);
+    return HX_OK;
+}
+
+void release(hx_ctx* c)
+{
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void* ptrs[] = {c->rho, c->ua, c->ub, c->rows, c->edges, c->acoef, c->bcoef, c->gsum, c->hdiag,
+                    c->hflip, c->vdiag, c->xi, c->counter, c->bath_off, c->error_flag, c->obs,
+                    c->trace_buf, c->energy_buf};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+hx::StageTables tables_of(const hx_ctx* c)
+{
+    hx::StageTables t{};
+    t.edges = c->edges;
+    t.acoef = c->acoef;
+    t.bcoef = c->bcoef;
+    t.gsum = c->gsum;
+    t.hdiag = c->hdiag;
+    t.hflip = c->hflip;
+    t.vdiag = c->vdiag;
+    t.xi = c->xi;
+    t.counter = c->counter;
+    t.bath_off = c->bath_off;
+    t.order = nullptr;
+    t.error_flag = c->error_flag;
+    t.H = c->H;
+    t.M = c->M;
+    t.J = c->J;
+    t.logd = c->logd;
+    return t;
+}
+
+// Enqueue one integrator step (Horner form of the order-m Taylor polynomial).
+int enqueue_step(hx_ctx* c)
+{
+    const hx::StageTables t = tables_of(c);
+    const int m = c->order;
+    if (m == 1) {
+        hx::launch_stage(t, c->rho, c->rho, c->ua, c->dt, hx::kBaseSelf, c->stream);
+        std::swap(c->rho, c->ua);
+    } else {
+        const double2* in = c->rho;
+        double2* bufs[2] = {c->ua, c->ub};
+        for (int s = 1; s <= m; ++s) {
+            const double alpha = c->dt / static_cast<double>(m - s + 1);
+            double2* out = (s == m) ? c->rho : bufs[(s - 1) & 1];
+            hx::launch_stage(t, in, c->rho, out, alpha, s == 1 ? hx::kBaseSelf : hx::kBaseRho, c->stream);
+            in = out;
+        }
+    }
+    c->counters.kernel_launches += m;
+    c->counters.stage_launches += m;
+    c->steps_done += 1;
+    return HX_OK;
+}
+
+int check_launch(const char* what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return hx::cuda_fail(e, what);
+    return HX_OK;
+}
+
+int read_error_flag(hx_ctx* c)
+{
+    int flag = 0;
+    HX_CUDA_TRY(cudaMemcpyAsync(&flag, c->error_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (flag != 0) {
+        cudaMemsetAsync(c->error_flag, 0, sizeof(int), c->stream);
+        return fail(HX_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration budget");
+    }
+    return HX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hx_hierarchy_tables(uint32_t modes, uint32_t max_depth, int32_t* rows, int32_t* edges, uint64_t count)
+{
+    uint64_t H = 0;
+    int rc = hx_hierarchy_size(modes, max_depth, &H);
+    if (rc != HX_OK) return rc;
+    if (count != H) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "count does not match hx_hierarchy_size");
+    if (H == 0) return HX_OK;
+    if (!rows || !edges) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL output buffer");
+    if (H >= (1ull << 31)) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "hierarchy exceeds int32 indexing");
+    cudaStream_t s = nullptr;
+    HX_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int32_t* dr = nullptr;
+    int32_t* de = nullptr;
+    cudaError_t e = cudaMalloc(&dr, H * modes * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&de, H * 2 * modes * sizeof(int32_t));
+    if (e != cudaSuccess) {
+        cudaFree(dr);
+        cudaStreamDestroy(s);
+        return hx::cuda_fail(e, "cudaMalloc tables");
+    }
+    rc = hx::build_tables_device(static_cast<int>(modes), static_cast<int>(max_depth), static_cast<long long>(H),
+                                 dr, de, s);
+    if (rc == HX_OK) {
+        e = cudaMemcpyAsync(rows, dr, H * modes * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(edges, de, H * 2 * modes * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = hx::cuda_fail(e, "copy tables to host");
+    }
+    cudaFree(dr);
+    cudaFree(de);
+    cudaStreamDestroy(s);
+    return rc;
+}
+
+int hx_ctx_create(const hx_problem* p, hx_ctx** out)
+{
+    if (!out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context output");
+    *out = nullptr;
+    if (!p) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL problem");
+    const uint32_t d = p->dim;
+    if (d < 2 || (d & (d - 1)) != 0)
+        return fail(HX_ERR_INVALID_DIMENSION, "dim must be a power of two >= 2");
+    int logd = 0;
+    while ((1u << logd) < d) ++logd;
+    if (logd > hx::kMaxLogD)
+        return fail(HX_ERR_UNSUPPORTED_EXECUTION, "fused FP64 path supports dim <= 64");
+    if (!p->h_diag) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "h_diag is NULL");
+    if (p->precision != HX_PRECISION_DOUBLE)
+        return fail(HX_ERR_UNSUPPORTED_PRECISION, "this entry point propagates in double precision only");
+    if (!(p->time_step > 0.0) || !std::isfinite(p->time_step))
+        return fail(HX_ERR_INVALID_RUNTIME_OPTION, "time_step must be positive");
+    if (p->integration_order < 1 || p->integration_order > 8)
+        return fail(HX_ERR_INVALID_RUNTIME_OPTION, "integration_order must be in 1..8");
+    if (p->n_baths == 0 || !p->baths) return fail(HX_ERR_UNSUPPORTED_BATH, "at least one bath is required");
+    if (p->n_baths > static_cast<uint32_t>(hx::kMaxBaths)) return fail(HX_ERR_UNSUPPORTED_BATH, "too many baths");
+    if (p->max_depth < 1) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "max_depth must be >= 1");
+    if (p->flags != 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "flags must be 0");
+
+    const int J = static_cast<int>(p->n_baths);
+    std::vector<hx::BathConst> bc(J);
+    int M = 0;
+    for (int j = 0; j < J; ++j) {
+        const hx_bath& b = p->baths[j];
+        if (!b.coupling_diag) return fail(HX_ERR_UNSUPPORTED_BATH, "bath coupling operator is NULL");
+        if (!(b.inverse_temperature > 0.0) || !(b.damping > 0.0) || !std::isfinite(b.coupling_strength))
+            return fail(HX_ERR_UNSUPPORTED_BATH, "bath needs positive beta and gamma and a finite coupling");
+        if (b.pade_terms > 32) return fail(HX_ERR_UNSUPPORTED_BATH, "too many Pade terms");
+        if (!hx::bath_constants(b.inverse_temperature, b.damping, b.coupling_strength,
+                                static_cast<int>(b.pade_terms), bc[j]))
+            return fail(HX_ERR_UNSUPPORTED_BATH, "bath coefficients are not finite (cot(beta gamma / 2) pole?)");
+        bc[j].offset = M;
+        M += static_cast<int>(b.pade_terms) + 1;
+    }
+    if (M > hx::kMaxModes) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "too many modes");
+    uint64_t H = 0;
+    int rc = hx_hierarchy_size(static_cast<uint32_t>(M), p->max_depth, &H);
+    if (rc != HX_OK) return rc;
+    if (H == 0 || H >= (1ull << 31)) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "hierarchy size out of range");
+
+    hx_ctx* c = new (std::nothrow) hx_ctx();
+    if (!c) return fail(HX_ERR_OUT_OF_MEMORY, "host allocation failed");
+    cudaGetDevice(&c->device);
+    c->d = static_cast<int>(d);
+    c->logd = logd;
+    c->M = M;
+    c->J = J;
+    c->H = static_cast<long long>(H);
+    c->order = static_cast<int>(p->integration_order);
+    c->dt = p->time_step;
+    c->slab = static_cast<size_t>(d) * d;
+
+    auto bail = [&](int code) {
+        release(c);
+        return code;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(hx::cuda_fail(e, "cudaStreamCreate"));
+    c->stream = c->own_stream;
+
+    const size_t nstate = static_cast<size_t>(H) * c->slab;
+    if ((rc = dev_alloc(c, &c->rho, nstate)) || (rc = dev_alloc(c, &c->ua, nstate)) ||
+        (rc = dev_alloc(c, &c->ub, nstate)) || (rc = dev_alloc(c, &c->rows, H * M)) ||
+        (rc = dev_alloc(c, &c->edges, H * 2 * M)) || (rc = dev_alloc(c, &c->acoef, H * M)) ||
+        (rc = dev_alloc(c, &c->bcoef, H * J)) || (rc = dev_alloc(c, &c->gsum, H)) ||
+        (rc = dev_alloc(c, &c->hdiag, d)) || (rc = dev_alloc(c, &c->hflip, logd)) ||
+        (rc = dev_alloc(c, &c->vdiag, static_cast<size_t>(J) * d)) || (rc = dev_alloc(c, &c->xi, J)) ||
+        (rc = dev_alloc(c, &c->counter, J)) || (rc = dev_alloc(c, &c->bath_off, J + 1)) ||
+        (rc = dev_alloc(c, &c->error_flag, 1)) || (rc = dev_alloc(c, &c->obs, 4)))
+        return bail(rc);
+
+    // host-side operator data
+    c->h_hdiag.assign(p->h_diag, p->h_diag + d);
+    c->h_hflip.assign(logd, 0.0);
+    if (p->h_flip) c->h_hflip.assign(p->h_flip, p->h_flip + logd);
+    std::vector<double> vd(static_cast<size_t>(J) * d), xi(J), ct(J), nu_m(M), phi_m(M, 0.0), tc(J), ta(J);
+    std::vector<int32_t> off(J + 1), mb(M), mk(M);
+    for (int j = 0; j < J; ++j) {
+        std::copy(p->baths[j].coupling_diag, p->baths[j].coupling_diag + d, vd.begin() + static_cast<size_t>(j) * d);
+        xi[j] = bc[j].xi;
+        ct[j] = bc[j].counter;
+        tc[j] = bc[j].theta_c;
+        ta[j] = bc[j].theta_a;
+        off[j] = bc[j].offset;
+        for (int k = 0; k <= bc[j].K; ++k) {
+            const int m = bc[j].offset + k;
+            mb[m] = j;
+            mk[m] = k;
+            nu_m[m] = bc[j].nu[k];
+            if (k >= 1) phi_m[m] = bc[j].phi[k - 1];
+        }
+    }
+    off[J] = M;
+    for (double v : vd)
+        if (!std::isfinite(v)) return bail(fail(HX_ERR_UNSUPPORTED_BATH, "coupling operator is not finite"));
+    for (double v : c->h_hdiag)
+        if (!std::isfinite(v)) return bail(fail(HX_ERR_INVALID_RUNTIME_OPTION, "h_diag is not finite"));
+
+    if ((rc = upload(c, c->hdiag, c->h_hdiag)) || (rc = upload(c, c->hflip, c->h_hflip)) ||
+        (rc = upload(c, c->vdiag, vd)) || (rc = upload(c, c->xi, xi)) || (rc = upload(c, c->counter, ct)) ||
+        (rc = upload(c, c->bath_off, off)))
+        return bail(rc);
+
+    // per-mode temporaries for the coefficient kernel
+    int32_t *dmb = nullptr, *dmk = nullptr;
+    double *dnu = nullptr, *dphi = nullptr, *dtc = nullptr, *dta = nullptr;
+    e = cudaMalloc(&dmb, M * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dmk, M * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dnu, M * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&dphi, M * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&dtc, J * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&dta, J * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dmb, mb.data(), M * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dmk, mk.data(), M * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dnu, nu_m.data(), M * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dphi, phi_m.data(), M * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dtc, tc.data(), J * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dta, ta.data(), J * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->error_flag, 0, sizeof(int), c->stream);
+    if (e != cudaSuccess) rc = hx::cuda_fail(e, "context setup");
+    if (rc == HX_OK) rc = hx::build_tables_device(M, static_cast<int>(p->max_depth), c->H, c->rows, c->edges, c->stream);
+    if (rc == HX_OK) {
+        hx::launch_coefficients(c->rows, c->H, M, J, dmb, dmk, dnu, dtc, dta, dphi, c->bath_off, c->acoef,
+                                c->bcoef, c->gsum, c->stream);
+        hx::launch_init_state(c->rho, static_cast<long long>(nstate), c->d, c->stream);
+        rc = check_launch("setup kernels");
+    }
+    if (rc == HX_OK) {
+        e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) rc = hx::cuda_fail(e, "context setup");
+    }
+    cudaFree(dmb);
+    cudaFree(dmk);
+    cudaFree(dnu);
+    cudaFree(dphi);
+    cudaFree(dtc);
+    cudaFree(dta);
+    if (rc != HX_OK) return bail(rc);
+    c->counters.kernel_launches += 3;
+    *out = c;
+    return HX_OK;
+}
+
+void hx_ctx_destroy(hx_ctx* ctx) { release(ctx); }
+
+int hx_ctx_set_stream(hx_ctx* c, void* stream)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+    return HX_OK;
+}
+
+int hx_ctx_get_stream(hx_ctx* c, void** stream)
+{
+    if (!c || !stream) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    *stream = c->stream;
+    return HX_OK;
+}
+
+int hx_ctx_info(const hx_ctx* c, hx_info* info)
+{
+    if (!c || !info) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    info->dim = static_cast<uint32_t>(c->d);
+    info->modes = static_cast<uint32_t>(c->M);
+    info->hierarchy_size = static_cast<uint64_t>(c->H);
+    info->state_bytes = static_cast<uint64_t>(c->H) * c->slab * sizeof(double2);
+    info->device_bytes = c->device_bytes;
+    info->steps_done = c->steps_done;
+    info->time = static_cast<double>(c->steps_done) * c->dt;
+    info->kernels_per_step = static_cast<uint32_t>(c->order);
+    return HX_OK;
+}
+
+int hx_ctx_counters(const hx_ctx* c, hx_counters* out)
+{
+    if (!c || !out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    *out = c->counters;
+    return HX_OK;
+}
+
+int hx_ctx_step(hx_ctx* c, uint64_t nsteps)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
+    for (uint64_t s = 0; s < nsteps; ++s) enqueue_step(c);
+    return check_launch("stage kernel launch");
+}
+
+int hx_ctx_sync(hx_ctx* c)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return read_error_flag(c);
+}
+
+int hx_ctx_step_trace(hx_ctx* c, uint64_t nsteps, double* rho0_trace, double* energy_trace)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
+    const int cap = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(nsteps, 1), 256));
+    if (c->trace_cap < cap) {
+        if (c->trace_buf) cudaFree(c->trace_buf);
+        if (c->energy_buf) cudaFree(c->energy_buf);
+        if (c->pinned) cudaFreeHost(c->pinned);
+        c->trace_buf = nullptr;
+        c->energy_buf = nullptr;
+        c->pinned = nullptr;
+        c->trace_cap = 0;
+        HX_CUDA_TRY(cudaMalloc(&c->trace_buf, cap * c->slab * sizeof(double2)));
+        HX_CUDA_TRY(cudaMalloc(&c->energy_buf, cap * 3 * sizeof(double)));
+        c->pinned_bytes = cap * (c->slab * sizeof(double2) + 3 * sizeof(double));
+        HX_CUDA_TRY(cudaMallocHost(&c->pinned, c->pinned_bytes));
+        c->trace_cap = cap;
+    }
+    double* pin_rho = c->pinned;
+    double* pin_en = c->pinned + static_cast<size_t>(c->trace_cap) * c->slab * 2;
+    uint64_t done = 0;
+    while (done < nsteps) {
+        const int chunk = static_cast<int>(std::min<uint64_t>(nsteps - done, c->trace_cap));
+        for (int t = 0; t < chunk; ++t) {
+            enqueue_step(c);
+            hx::launch_observables(c->rho, c->logd, c->hdiag, c->hflip,
+                                   rho0_trace ? c->trace_buf + static_cast<size_t>(t) * c->slab : nullptr,
+                                   c->energy_buf + 3 * t, c->stream);
+            c->counters.kernel_launches += 1;
+        }
+        int rc = check_launch("trace step");
+        if (rc != HX_OK) return rc;
+        if (rho0_trace) {
+            HX_CUDA_TRY(cudaMemcpyAsync(pin_rho, c->trace_buf, chunk * c->slab * sizeof(double2),
+                                        cudaMemcpyDeviceToHost, c->stream));
+            c->counters.d2h_bytes += chunk * c->slab * sizeof(double2);
+        }
+        if (energy_trace) {
+            HX_CUDA_TRY(cudaMemcpyAsync(pin_en, c->energy_buf, chunk * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                        c->stream));
+            c->counters.d2h_bytes += chunk * 3 * sizeof(double);
+        }
+        HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (rho0_trace)
+            std::memcpy(rho0_trace + done * c->slab * 2, pin_rho, chunk * c->slab * sizeof(double2));
+        if (energy_trace)
+            for (int t = 0; t < chunk; ++t) energy_trace[done + t] = pin_en[3 * t];
+        done += chunk;
+    }
+    return read_error_flag(c);
+}
+
+int hx_ctx_read_rho0(hx_ctx* c, double* out, uint64_t n)
+{
+    if (!c || !out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    if (n < 2 * c->slab) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "output buffer too small");
+    HX_CUDA_TRY(cudaMemcpyAsync(out, c->rho, c->slab * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->counters.d2h_bytes += c->slab * sizeof(double2);
+    return read_error_flag(c);
+}
+
+int hx_ctx_observables(hx_ctx* c, double* energy, double* trace_re, double* trace_im)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
+    hx::launch_observables(c->rho, c->logd, c->hdiag, c->hflip, nullptr, c->obs, c->stream);
+    c->counters.kernel_launches += 1;
+    int rc = check_launch("observables kernel");
+    if (rc != HX_OK) return rc;
+    double h[3];
+    HX_CUDA_TRY(cudaMemcpyAsync(h, c->obs, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (energy) *energy = h[0];
+    if (trace_re) *trace_re = h[1];
+    if (trace_im) *trace_im = h[2];
+    return read_error_flag(c);
+}
+
+int hx_ctx_read_state(hx_ctx* c, double* out, uint64_t n)
+{
+    if (!c || !out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    const size_t count = static_cast<size_t>(c->H) * c->slab;
+    if (n < 2 * count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "output buffer too small");
+    HX_CUDA_TRY(cudaMemcpyAsync(out, c->rho, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->counters.d2h_bytes += count * sizeof(double2);
+    return read_error_flag(c);
+}
+
+int hx_ctx_write_state(hx_ctx* c, const double* in, uint64_t n)
+{
+    if (!c || !in) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    const size_t count = static_cast<size_t>(c->H) * c->slab;
+    if (n < 2 * count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "input buffer too small");
+    HX_CUDA_TRY(cudaMemcpyAsync(c->rho, in, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    c->counters.h2d_bytes += count * sizeof(double2);
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return HX_OK;
+}
+
+int hx_ctx_state_device_ptr(hx_ctx* c, void** ptr)
+{
+    if (!c || !ptr) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    *ptr = c->rho;
+    return HX_OK;
+}
+
+int hx_ctx_rhs(hx_ctx* c, double* out, uint64_t n)
+{
+    if (!c || !out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    const size_t count = static_cast<size_t>(c->H) * c->slab;
+    if (n < 2 * count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "output buffer too small");
+    hx::launch_stage(tables_of(c), c->rho, c->rho, c->ua, 1.0, hx::kBaseZero, c->stream);
+    c->counters.kernel_launches += 1;
+    int rc = check_launch("stage kernel launch");
+    if (rc != HX_OK) return rc;
+    HX_CUDA_TRY(cudaMemcpyAsync(out, c->ua, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return read_error_flag(c);
+}
+
+int hx_ctx_check_finite(hx_ctx* c)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
+    int host = 0;
+    int* scratch = reinterpret_cast<int*>(c->obs + 3);
+    HX_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(int), c->stream));
+    hx::launch_finite_check(c->rho, static_cast<long long>(c->H) * c->slab, scratch, c->stream);
+    c->counters.kernel_launches += 1;
+    int rc = check_launch("finite check");
+    if (rc != HX_OK) return rc;
+    HX_CUDA_TRY(cudaMemcpyAsync(&host, scratch, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (host != 0) return fail(HX_ERR_NON_FINITE, "state holds non-finite values");
+    return read_error_flag(c);
+}
+
+}  // extern "C"

@@ -1,0 +1,133 @@
+// Internal declarations of the helix_b200 CUDA library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "helix_b200.h"
+
+namespace hx {
+
+// Thread-local last-error text behind hx_last_error().
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define HX_CUDA_TRY(expr)                                     \
+    do {                                                      \
+        cudaError_t hx_e_ = (expr);                           \
+        if (hx_e_ != cudaSuccess) return ::hx::cuda_fail(hx_e_, #expr); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Host math (hx_host.cpp)
+// ---------------------------------------------------------------------------
+
+// [K-1/K] Pade poles/residues of the Bose function (src/psd/psd.cu:12-113).
+bool psd_bose(int K, double* poles, double* residues);
+
+// Per-bath constants of the right-hand side, in the reference's form
+// (src/initialize.cu:160-218, omega0 = 1):
+//   nu[k]      nu_0 = gamma, nu_k = xi_k / beta
+//   theta_c    Im KThetaCommutate   = (beta gamma/2) cot(beta gamma/2) zeta/beta
+//   theta_a    KThetaAntiCommutate  = (beta gamma/2) zeta / beta
+//   phi[k-1]   Im KPhi_k            = (zeta/beta) 2 eta_k gamma^2 / (nu_k^2 - gamma^2)
+//   xi         KXi (real)           = sigma zeta / beta
+//   counter    Im KXiCounter        = zeta (beta gamma/2) / beta
+struct BathConst {
+    int K = 0;
+    int offset = 0;  // first mode index
+    std::vector<double> nu, phi;
+    double theta_c = 0, theta_a = 0, xi = 0, counter = 0;
+};
+bool bath_constants(double beta, double gamma, double zeta, int K, BathConst& out);
+
+uint64_t binom_u64(int n, int k);
+
+// ---------------------------------------------------------------------------
+// Device-side parameter blocks
+// ---------------------------------------------------------------------------
+
+constexpr int kMaxLogD = 6;       // fused FP64 stage kernel: d <= 64
+constexpr int kMaxModes = 128;
+constexpr int kMaxBaths = 64;
+
+// Read-only per-context tables used by the stage kernel.
+struct StageTables {
+    const int32_t* edges;    // [H][2M] reference layout, sentinel H
+    const double* acoef;     // [H][M]  down-commutator weight a_{n,m}
+    const double* bcoef;     // [H][J]  down anti-commutator weight b_{n,j} (Drude mode)
+    const double* gsum;      // [H]     sum_m nu_m n_m
+    const double* hdiag;     // [d]
+    const double* hflip;     // [log2 d]
+    const double* vdiag;     // [J][d]
+    const double* xi;        // [J]
+    const double* counter;   // [J]
+    const int32_t* bath_off; // [J+1]  mode offsets
+    const int32_t* order;    // [H] processing order (ADO index per CTA), or nullptr
+    int* error_flag;         // device error word
+    long long H;
+    int M, J, logd;
+};
+
+enum BaseKind : int { kBaseSelf = 0, kBaseRho = 1, kBaseZero = 2 };
+
+// out_n = base_n + alpha * L(u)_n for every ADO n
+void launch_stage(const StageTables& t, const double2* u, const double2* rho, double2* out,
+                  double alpha, int base_kind, cudaStream_t s);
+
+// Tables on the device (hx_tables.cu)
+int build_tables_device(int M, int D, long long H, int32_t* d_rows, int32_t* d_edges, cudaStream_t s);
+void launch_coefficients(const int32_t* rows, long long H, int M, int J, const int32_t* mode_bath,
+                         const int32_t* mode_k, const double* nu, const double* theta_c,
+                         const double* theta_a, const double* phi, const int32_t* bath_off,
+                         double* acoef, double* bcoef, double* gsum, cudaStream_t s);
+
+// Observables of rho_0: energy = Re Tr(H rho_0), trace.  Optionally copies
+// rho_0 into rho0_copy.  out[0] = energy, out[1] = Re tr, out[2] = Im tr.
+void launch_observables(const double2* rho0, int logd, const double* hdiag, const double* hflip,
+                        double2* rho0_copy, double* out, cudaStream_t s);
+
+void launch_finite_check(const double2* x, long long n, int* flag, cudaStream_t s);
+void launch_init_state(double2* rho, long long n, int d, cudaStream_t s);
+
+}  // namespace hx
+
+struct hx_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int d = 0, logd = 0, M = 0, J = 0, order = 4;
+    long long H = 0;
+    double dt = 0.0;
+    uint64_t steps_done = 0;
+    size_t slab = 0;   // d*d
+    // device memory
+    double2* rho = nullptr;
+    double2* ua = nullptr;
+    double2* ub = nullptr;
+    int32_t* rows = nullptr;
+    int32_t* edges = nullptr;
+    double* acoef = nullptr;
+    double* bcoef = nullptr;
+    double* gsum = nullptr;
+    double* hdiag = nullptr;
+    double* hflip = nullptr;
+    double* vdiag = nullptr;
+    double* xi = nullptr;
+    double* counter = nullptr;
+    int32_t* bath_off = nullptr;
+    int* error_flag = nullptr;
+    double* obs = nullptr;        // [3] observables scratch
+    double2* trace_buf = nullptr; // per-step rho_0 chunk
+    double* energy_buf = nullptr;
+    int trace_cap = 0;
+    double* pinned = nullptr;     // pinned staging for traces
+    size_t pinned_bytes = 0;
+    size_t device_bytes = 0;
+    hx_counters counters{};
+    std::vector<double> h_hdiag, h_hflip;
+};

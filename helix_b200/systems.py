@@ -1,0 +1,267 @@
+"""Problem setup on the host: spin-glass and legacy systems, seeded instances.
+
+The reference builds its operators on the host in ``src/initialize.cu``
+(``createSystem``, :319-333) and ``src/initialize_detail.h`` (:100-157).  This
+module builds the same kinds of objects in plain Python/numpy for the C-ABI:
+
+* ``spin_glass`` — the transverse-field Ising spin glass
+  H = sum_{i<j} J_ij sz_i sz_j + h sum_i sx_i with one Drude-Lorentz bath per
+  spin coupled through V_i = sz_i (Pauli, eigenvalues +-1).
+* ``legacy_spin_glass`` — the reference's compiled model (diagonal H with the
+  legacy accumulation, one collective bath, V = Dlong*sum s_z + Dtrans*flips).
+
+Conventions (shared with the oracle): spin i <-> bit i of the basis index,
+"up" = bit 1 = sz eigenvalue +1; the initial state is |d-1><d-1| (all up), as
+in ``buildInitialRho`` (src/initialize.cu:287-301).
+
+The seeded generator is splitmix64 with Box-Muller normals, written here so
+every consumer (CUDA path, oracle, C++ API) sees the same J_ij.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+MASK64 = (1 << 64) - 1
+
+
+class SplitMix64:
+    """splitmix64 stream; uniform() in [0,1) from the top 53 bits."""
+
+    def __init__(self, seed: int):
+        self.state = seed & MASK64
+
+    def next_u64(self) -> int:
+        self.state = (self.state + 0x9E3779B97F4A7C15) & MASK64
+        z = self.state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK64
+        return z ^ (z >> 31)
+
+    def uniform(self) -> float:
+        return (self.next_u64() >> 11) * (1.0 / 9007199254740992.0)
+
+    def normal(self) -> float:
+        """Box-Muller, cosine branch only: two uniforms per normal."""
+        u1 = 1.0 - self.uniform()  # (0, 1]
+        u2 = self.uniform()
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+    def uniform_range(self, lo: float, hi: float) -> float:
+        return lo + (hi - lo) * self.uniform()
+
+    def randint(self, lo: int, hi: int) -> int:
+        """Uniform integer in [lo, hi]."""
+        return lo + int(self.uniform() * (hi - lo + 1))
+
+
+def seeded_couplings(n_spins: int, seed: int) -> np.ndarray:
+    """J (n x n, symmetric, zero diagonal), J_ij ~ N(0,1) drawn for i<j in row-major pair order."""
+    rng = SplitMix64(seed)
+    J = np.zeros((n_spins, n_spins))
+    for i in range(n_spins):
+        for j in range(i + 1, n_spins):
+            J[i, j] = J[j, i] = rng.normal()
+    return J
+
+
+def spin_signs(n_spins: int) -> np.ndarray:
+    """s[i, r] = +1 if bit i of r is set else -1."""
+    d = 1 << n_spins
+    r = np.arange(d)
+    return np.stack([np.where((r >> i) & 1, 1.0, -1.0) for i in range(n_spins)])
+
+
+@dataclass
+class BathSpec:
+    """Drude-Lorentz bath with Pade K terms, in the reference's units.
+
+    ``zeta`` is the reference's ``Param::Zeta`` (``Bath::couplingStrength``);
+    the reorganisation energy is lambda = zeta*gamma/2 (omega0 = 1,
+    src/initialize.cu:204-218).  ``v_diag`` is the diagonal of the coupling
+    operator V (None when ``v_csr`` gives a general operator).
+    """
+
+    beta: float
+    gamma: float
+    zeta: float
+    K: int
+    v_diag: np.ndarray | None = None
+    v_csr: tuple | None = None  # (ptr, col, val complex) for non-diagonal V
+
+    @staticmethod
+    def drude_lorentz(lam: float, gamma: float, temperature: float, K: int, v_diag=None, v_csr=None):
+        return BathSpec(beta=1.0 / temperature, gamma=gamma, zeta=2.0 * lam / gamma, K=K,
+                        v_diag=None if v_diag is None else np.asarray(v_diag, dtype=np.float64),
+                        v_csr=v_csr)
+
+    @property
+    def lam(self) -> float:
+        return 0.5 * self.zeta * self.gamma
+
+
+@dataclass
+class Problem:
+    """One HEOM instance: H = diag(h_diag) + sum_i h_flip[i] sx_i, baths, truncation."""
+
+    dim: int
+    h_diag: np.ndarray
+    h_flip: np.ndarray
+    baths: list[BathSpec]
+    max_depth: int                  # exclusive bound on sum(n) (reference semantics)
+    dt: float
+    name: str = ""
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_spins(self) -> int:
+        return int(round(math.log2(self.dim)))
+
+    @property
+    def modes(self) -> int:
+        return sum(b.K + 1 for b in self.baths)
+
+    def hierarchy_size(self) -> int:
+        return hierarchy_size(self.modes, self.max_depth)
+
+    def h_csr(self):
+        """H as CSR (ptr, col, complex val), row-major, columns ascending."""
+        d = self.dim
+        n = self.n_spins
+        ptr = [0]
+        col: list[int] = []
+        val: list[complex] = []
+        for r in range(d):
+            entries = {r: complex(self.h_diag[r])}
+            for i in range(n):
+                if self.h_flip[i] != 0.0:
+                    entries[r ^ (1 << i)] = entries.get(r ^ (1 << i), 0.0) + complex(self.h_flip[i])
+            for c in sorted(entries):
+                col.append(c)
+                val.append(entries[c])
+            ptr.append(len(col))
+        return np.array(ptr, np.int32), np.array(col, np.int32), np.array(val, np.complex128)
+
+    def h_dense(self) -> np.ndarray:
+        ptr, col, val = self.h_csr()
+        m = np.zeros((self.dim, self.dim), np.complex128)
+        for r in range(self.dim):
+            m[r, col[ptr[r]:ptr[r + 1]]] = val[ptr[r]:ptr[r + 1]]
+        return m
+
+    def bath_csr(self, j: int):
+        b = self.baths[j]
+        if b.v_csr is not None:
+            ptr, col, val = b.v_csr
+            return np.asarray(ptr, np.int32), np.asarray(col, np.int32), np.asarray(val, np.complex128)
+        d = self.dim
+        return (np.arange(d + 1, dtype=np.int32), np.arange(d, dtype=np.int32),
+                np.asarray(b.v_diag, np.float64).astype(np.complex128))
+
+
+def hierarchy_size(modes: int, max_depth: int) -> int:
+    """C(modes + max_depth - 1, modes): index vectors with sum(n) < max_depth."""
+    if max_depth <= 0:
+        return 0
+    return math.comb(modes + max_depth - 1, modes)
+
+
+def spin_glass(n_spins: int, seed: int, h: float = 1.0, lam: float = 0.1, gamma: float = 1.0,
+               temperature: float = 1.0, K: int = 2, depth: int = 3, dt: float = 0.01,
+               J: np.ndarray | None = None) -> Problem:
+    """Transverse-field Ising spin glass with one sz bath per spin.
+
+    ``depth`` is the hierarchy depth L (sum(n) <= L); the reference's exclusive
+    ``maxDepth`` is L + 1.
+    """
+    if J is None:
+        J = seeded_couplings(n_spins, seed)
+    s = spin_signs(n_spins)
+    d = 1 << n_spins
+    E = np.zeros(d)
+    for i in range(n_spins):
+        for j in range(i + 1, n_spins):
+            E += J[i, j] * s[i] * s[j]
+    baths = [BathSpec.drude_lorentz(lam, gamma, temperature, K, v_diag=s[i]) for i in range(n_spins)]
+    return Problem(dim=d, h_diag=E, h_flip=np.full(n_spins, float(h)), baths=baths,
+                   max_depth=depth + 1, dt=dt, name=f"spin_glass_n{n_spins}_L{depth}_K{K}",
+                   meta={"seed": seed, "J": J, "h": h, "lam": lam, "T": temperature, "depth": depth})
+
+
+# Legacy compiled-model constants (src/parameters.cu:11-31)
+LEGACY = dict(omega0=1.0, dlong=1.0, dtrans=1.0, jnaver=0.6, beta=3.0, gamma=1.0, zeta=0.01,
+              K=2, jmax=3, dt=0.1)
+
+
+def legacy_coupling_matrix(n: int, value: float) -> np.ndarray:
+    """Nearest-neighbour chain (buildCouplingMatrix for spinCount != 9, initialize_detail.h:51-60)."""
+    if n == 9:
+        raise NotImplementedError("9-spin lattices are outside the supported legacy shapes")
+    c = np.zeros((n, n))
+    for i in range(n):
+        for j in range(n):
+            if abs(i - j) == 1:
+                c[i, j] = value
+    return c
+
+
+def legacy_h_diagonal(dim: int) -> np.ndarray:
+    """Diagonal of the legacy H: sum of projections plus sum_{k<j} J_jk p_j p_k
+    with p = +-omega0/2 (hamiltonianDiagonal, initialize_detail.h:143-157)."""
+    n = int(round(math.log2(dim)))
+    cm = legacy_coupling_matrix(n, LEGACY["jnaver"])
+    out = np.zeros(dim)
+    for state in range(dim):
+        p = [0.5 * LEGACY["omega0"] if (state >> s) & 1 else -0.5 * LEGACY["omega0"] for s in range(n)]
+        total = 0.0
+        for x in p:
+            total += x
+        for j in range(n):
+            for k in range(j):
+                total += cm[j, k] * p[j] * p[k]
+        out[state] = total
+    return out
+
+
+def legacy_sparse_flip(mask: int) -> bool:
+    """isSparseFlipMask (initialize_detail.h:38-44): masks 1..256; 512 is absent."""
+    return mask in (1, 2, 4, 8, 16, 32, 64, 128, 256)
+
+
+def legacy_v_csr(dim: int):
+    """Legacy sparse V: diagonal Dlong*sum(p), Dtrans at sparse flip masks
+    (buildSparseOperators, initialize.cu:95-147); columns in ascending order."""
+    n = int(round(math.log2(dim)))
+    ptr = [0]
+    col: list[int] = []
+    val: list[complex] = []
+    for row in range(dim):
+        psum = 0.0
+        for s in range(n):
+            psum += 0.5 * LEGACY["omega0"] if (row >> s) & 1 else -0.5 * LEGACY["omega0"]
+        for c in range(dim):
+            if c == row:
+                col.append(c)
+                val.append(complex(LEGACY["dlong"] * psum))
+            if legacy_sparse_flip(row ^ c):
+                col.append(c)
+                val.append(complex(LEGACY["dtrans"]))
+        ptr.append(len(col))
+    return np.array(ptr, np.int32), np.array(col, np.int32), np.array(val, np.complex128)
+
+
+def legacy_spin_glass(dim: int = 1024, dt: float | None = None) -> Problem:
+    """The reference's compiled model at Hilbert size ``dim`` (default 1024)."""
+    L = LEGACY
+    bath = BathSpec(beta=L["beta"], gamma=L["gamma"], zeta=L["zeta"], K=L["K"], v_csr=legacy_v_csr(dim))
+    n = int(round(math.log2(dim)))
+    return Problem(dim=dim, h_diag=legacy_h_diagonal(dim), h_flip=np.zeros(n), baths=[bath],
+                   max_depth=L["jmax"], dt=L["dt"] if dt is None else dt, name=f"legacy_d{dim}")
+
+
+def initial_rho0(dim: int) -> np.ndarray:
+    rho = np.zeros((dim, dim), np.complex128)
+    rho[dim - 1, dim - 1] = 1.0
+    return rho

@@ -1,0 +1,196 @@
+/* helix_b200 — C ABI of the B200 HEOM propagator.
+ *
+ * This is the drop-in boundary for the reference's propagation path
+ * (HELIX: helix::HEOMSolver().run(system, hierarchy, options) -> RunResult).
+ * Plain C types only: pointers, sizes and status codes.  The C++ helix:: API
+ * in include/helix/ is a thin layer over these entry points, and Python binds
+ * them with ctypes (helix_b200/capi.py).
+ *
+ * Conventions
+ *  - Every function returns HX_OK (0) or 1 + the helix::StatusCode value of
+ *    the failure (include/helix/types.h; codes are append-only).  The text of
+ *    the last failure on the calling thread is hx_last_error().
+ *  - Complex buffers are interleaved (re, im) doubles, matrices row-major.
+ *  - A context owns all device memory it uses and runs its work on one CUDA
+ *    stream (hx_ctx_set_stream can substitute the caller's stream).  A
+ *    context may be driven by one host thread at a time; several contexts
+ *    may live on one device.
+ *  - Hierarchy truncation uses the reference semantics: index vectors n with
+ *    sum(n) < max_depth (exclusive bound; depth L <=> max_depth = L + 1).
+ *  - Mode order is bath-major: mode = sum_{i<j}(K_i + 1) + k, k = 0 the Drude
+ *    mode of bath j, k >= 1 its Pade modes.
+ */
+#ifndef HELIX_B200_H
+#define HELIX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HX_OK 0
+/* 1 + helix::StatusCode (include/helix/types.h) */
+#define HX_ERR_INVALID_DIMENSION 1
+#define HX_ERR_INVALID_RUNTIME_OPTION 6
+#define HX_ERR_UNSUPPORTED_PRECISION 7
+#define HX_ERR_UNSUPPORTED_EXECUTION 10
+#define HX_ERR_UNSUPPORTED_BATH 11
+#define HX_ERR_UNSUPPORTED_HIERARCHY 12
+#define HX_ERR_BATH_EXPONENTS_INVALID 14
+#define HX_ERR_CUDA 15          /* StatusCode::CudaFailure (appended) */
+#define HX_ERR_OUT_OF_MEMORY 16 /* StatusCode::OutOfMemory (appended) */
+#define HX_ERR_NON_FINITE 17    /* StatusCode::NonFiniteState (appended) */
+#define HX_ERR_DEVICE_TIMEOUT 18 /* StatusCode::DeviceWaitTimeout (appended) */
+
+#define HX_PRECISION_SINGLE 0
+#define HX_PRECISION_DOUBLE 1
+
+/* One Drude-Lorentz bath with Pade terms, coupled through a diagonal system
+ * operator V_j.  Replaces the compiled bath of the reference
+ * (src/parameters.cu:25-31; Bath, include/helix/types.h:108-128). */
+typedef struct hx_bath {
+    double inverse_temperature; /* beta (Param::Betah) */
+    double damping;             /* gamma (Param::Gamma) */
+    double coupling_strength;   /* zeta (Param::Zeta); lambda = zeta*gamma/2 */
+    uint32_t pade_terms;        /* K (Param::KMax) */
+    const double* coupling_diag; /* dim real values: diagonal of V_j */
+} hx_bath;
+
+/* One HEOM problem.  H = diag(h_diag) + sum_i h_flip[i] * sigma_x(spin i),
+ * spin i <-> bit i of the basis index.  Replaces initialize()
+ * (src/initialize.cu:342-353) and the compiled parameters it reads. */
+typedef struct hx_problem {
+    uint32_t dim;               /* Hilbert dimension d = 2^spins, 2 <= d <= 64 */
+    const double* h_diag;       /* d diagonal entries of H */
+    const double* h_flip;       /* log2(d) transverse-field coefficients, or NULL */
+    uint32_t n_baths;
+    const hx_bath* baths;
+    uint32_t max_depth;         /* exclusive bound on sum(n) */
+    double time_step;           /* dt (Param::Step) */
+    uint32_t integration_order; /* Taylor order (Param::IntegrationNum), 1..8 */
+    uint32_t precision;         /* HX_PRECISION_DOUBLE */
+    uint32_t flags;             /* reserved, 0 */
+} hx_problem;
+
+typedef struct hx_info {
+    uint32_t dim;
+    uint32_t modes;
+    uint64_t hierarchy_size;    /* number of ADOs */
+    uint64_t state_bytes;       /* bytes of one full hierarchy state */
+    uint64_t device_bytes;      /* device memory the context holds */
+    uint64_t steps_done;
+    double time;                /* steps_done * dt */
+    uint32_t kernels_per_step;  /* kernel launches one step enqueues */
+} hx_info;
+
+/* Profiling counters (replaces src/library/backend_profiling.cpp:9-137). */
+typedef struct hx_counters {
+    uint64_t kernel_launches;
+    uint64_t stage_launches;
+    uint64_t h2d_bytes;
+    uint64_t d2h_bytes;
+} hx_counters;
+
+typedef struct hx_ctx hx_ctx;
+
+/* Text of the last failure on this thread ("" if none). */
+const char* hx_last_error(void);
+
+/* Library version string. (helix::runtimeVersion, src/helix.cpp:18-21) */
+const char* hx_version(void);
+
+/* Number of ADOs for `modes` modes and exclusive depth bound `max_depth`.
+ * (hierarchySizeFor, src/initialize_detail.h:159-172) */
+int hx_hierarchy_size(uint32_t modes, uint32_t max_depth, uint64_t* count);
+
+/* Hierarchy index rows (count x modes) and neighbour edges (count x 2*modes)
+ * in the reference order and sentinel convention, built on the device and
+ * copied to the caller's host buffers: rows in lexicographic order with mode
+ * 0 most significant, edges[i][k] = index of n_i + e_k, edges[i][modes + k] =
+ * index of n_i - e_k, sentinel = count.  `count` must equal
+ * hx_hierarchy_size().  (buildHierarchyRows / buildHierarchyEdges,
+ * src/initialize_detail.h:174-269; initializeHierarchyStorage,
+ * src/initialize.cu:237-250) */
+int hx_hierarchy_tables(uint32_t modes, uint32_t max_depth, int32_t* rows, int32_t* edges,
+                        uint64_t count);
+
+/* Pade poles xi_k and residues eta_k (k < K) of the Bose function, [K-1/K].
+ * (getPsdPoleResidue, src/psd/psd.cu:12-113) */
+int hx_psd(uint32_t K, double* poles, double* residues);
+
+/* Seeded J_ij ~ N(0,1) for i<j in row-major pair order (splitmix64 +
+ * Box-Muller), written symmetric into J (n x n, zero diagonal).  Synthetic
+ * instance generator; no counterpart in the reference. */
+int hx_seeded_couplings(uint32_t n_spins, uint64_t seed, double* J);
+
+/* Create a context on the current CUDA device: builds tables and
+ * coefficients on the device, allocates the state and sets rho to the
+ * reference initial state |d-1><d-1| with all other ADOs zero.
+ * (initialize(), src/initialize.cu:342-353; LegacyRuntimeSession::create,
+ * src/library/legacy_runtime_session.cu:53-77) */
+int hx_ctx_create(const hx_problem* problem, hx_ctx** out);
+
+/* Release every device resource of the context.
+ * (LegacyRuntimeSession::destroy, src/library/legacy_runtime_session.cu:108-118;
+ * clearLiouvilleStorage, src/liouville.cu:871-920) */
+void hx_ctx_destroy(hx_ctx* ctx);
+
+/* Use `stream` (a cudaStream_t; NULL = the context's own stream) for all
+ * further work of the context. */
+int hx_ctx_set_stream(hx_ctx* ctx, void* stream);
+int hx_ctx_get_stream(hx_ctx* ctx, void** stream);
+
+int hx_ctx_info(const hx_ctx* ctx, hx_info* info);
+int hx_ctx_counters(const hx_ctx* ctx, hx_counters* counters);
+
+/* Enqueue `nsteps` integrator steps on the context stream (asynchronous).
+ * (develop() loop, src/liouville.cu:502-590;
+ * LegacyRuntimeSession::run_steps, src/library/legacy_runtime_session.cu:79-100) */
+int hx_ctx_step(hx_ctx* ctx, uint64_t nsteps);
+
+/* As hx_ctx_step, and after every step write rho_0 (d*d complex) to
+ * rho0_trace[step] and Tr(H rho_0) to energy_trace[step] (either may be NULL).
+ * Host buffers; the call returns when the last values have landed.
+ * (ResultMode::ObservableTrace, validation-only in the reference,
+ * src/helix.cpp:315-319; energy as in src/cli_compatibility.cu:80-98) */
+int hx_ctx_step_trace(hx_ctx* ctx, uint64_t nsteps, double* rho0_trace, double* energy_trace);
+
+/* Wait for all work of the context. */
+int hx_ctx_sync(hx_ctx* ctx);
+
+/* Copy rho_0 (d*d complex, row-major) into a host buffer of n doubles
+ * (n >= 2*d*d).  (ResultExtractor::final_reduced_density,
+ * src/library/result_extractor.cu:35-90) */
+int hx_ctx_read_rho0(hx_ctx* ctx, double* out, uint64_t n);
+
+/* Tr(H rho_0) and Tr(rho_0) computed on the device.
+ * (energyFromDensityDiagonal, src/library/energy_observable.cpp:8-39,
+ * generalised to the off-diagonal H) */
+int hx_ctx_observables(hx_ctx* ctx, double* energy, double* trace_re, double* trace_im);
+
+/* Full hierarchy state (hierarchy_size * d * d complex) to / from host
+ * memory, reference ADO order.  (snapshot writer / loader,
+ * src/cli_compatibility.cu:130-145, src/initialize.cu:266-285) */
+int hx_ctx_read_state(hx_ctx* ctx, double* out, uint64_t n);
+int hx_ctx_write_state(hx_ctx* ctx, const double* in, uint64_t n);
+
+/* Device pointer of the state (hierarchy_size * d * d double2), for callers
+ * that fill or read it on the device. */
+int hx_ctx_state_device_ptr(hx_ctx* ctx, void** ptr);
+
+/* One evaluation of the right-hand side L(rho) of the current state into a
+ * host buffer (hierarchy_size * d * d complex).  Test hook for parity of the
+ * fused kernel against the reference RHS (getdRhoSparse, src/liouville.cu:749-869). */
+int hx_ctx_rhs(hx_ctx* ctx, double* out, uint64_t n);
+
+/* Device check that the state holds only finite values; returns
+ * HX_ERR_NON_FINITE otherwise. */
+int hx_ctx_check_finite(hx_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HELIX_B200_H */

@@ -1,0 +1,79 @@
+"""CPU tests of the C-ABI library: it loads, exports every declared symbol,
+and its host-side entry points and validation behave (no device calls)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from helix_b200 import capi
+from helix_b200 import systems as S
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "helix_b200.h")).read()
+    return sorted(set(re.findall(r"\b(hx_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_exports_every_declared_symbol():
+    lib = capi.lib()
+    declared = _declared()
+    assert declared == sorted(capi.EXPORTS)
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_version_and_sizes():
+    assert capi.version().startswith("helix_b200")
+    for M, D in [(12, 4), (18, 5), (3, 3), (16, 4), (15, 6)]:
+        assert capi.hierarchy_size(M, D) == O.lib().or_hierarchy_size(M, D)
+    assert capi.hierarchy_size(5, 0) == 0
+
+
+def test_psd_bit_exact_against_reference_code(golden):
+    for case in golden("reference_psd.json")["cases"]:
+        p, r = capi.psd(case["K"])
+        np.testing.assert_array_equal(p, np.array(case["poles"]))
+        np.testing.assert_array_equal(r, np.array(case["residues"]))
+
+
+def _status_of(problem, **override):
+    try:
+        ctx = capi.Context(problem, **override)
+        ctx.close()
+        return None
+    except capi.HxError as e:
+        return e.status
+
+
+def test_validation_errors_before_any_device_call():
+    good = S.spin_glass(2, seed=1, depth=2, K=1)
+    bad_dim = S.spin_glass(2, seed=1, depth=2, K=1)
+    bad_dim.dim = 3
+    assert _status_of(bad_dim) == "InvalidDimension"
+    big = S.spin_glass(7, seed=1, depth=1, K=0)
+    assert _status_of(big) == "UnsupportedExecution"
+    nodepth = S.spin_glass(2, seed=1, depth=2, K=1)
+    nodepth.max_depth = 0
+    assert _status_of(nodepth) == "UnsupportedHierarchy"
+    nobath = S.spin_glass(2, seed=1, depth=2, K=1)
+    nobath.baths = []
+    with pytest.raises(Exception):
+        capi.Context(nobath)
+    assert _status_of(good, order=0) == "InvalidRuntimeOption"
+    assert _status_of(good, dt=-1.0) == "InvalidRuntimeOption"
+    hot = S.spin_glass(2, seed=1, depth=2, K=1)
+    hot.baths[0].gamma = -1.0
+    assert _status_of(hot) == "UnsupportedBath"
+
+
+def test_last_error_text_is_thread_local_string():
+    try:
+        capi.hierarchy_size(0, 3)
+    except capi.HxError as e:
+        assert "mode" in str(e)
+    assert isinstance(capi.lib().hx_last_error(), bytes)

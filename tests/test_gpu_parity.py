@@ -1,0 +1,207 @@
+"""GPU parity of the fused sm_100a propagator against the FP64 oracle.
+
+Bars: hierarchy tables bit-exact; rho_0(t) and <H>(t) within 1e-10 max-abs
+(FP64 mode); single RHS evaluations within 1e-12 of the oracle's scale.
+All calls go through the C ABI (helix_b200/capi.py -> libhelix_b200.so).
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from helix_b200 import capi
+from helix_b200 import systems as S
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10  # FP64 max-abs bar for rho_0 and energy
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, np.int32).tobytes()).hexdigest()
+
+
+def test_device_tables_bit_exact(golden):
+    g = golden("reference_tables.json")
+    for case in g["small"]:
+        rows, edges = capi.hierarchy_tables(case["modes"], case["max_depth"])
+        np.testing.assert_array_equal(rows, np.array(case["rows"], np.int32).reshape(rows.shape))
+        np.testing.assert_array_equal(edges, np.array(case["edges"], np.int32).reshape(edges.shape))
+    for case in g["large"]:
+        rows, edges = capi.hierarchy_tables(case["modes"], case["max_depth"])
+        assert rows.shape[0] == case["count"]
+        assert _sha(rows) == case["rows_sha256"]
+        assert _sha(edges) == case["edges_sha256"]
+
+
+def test_device_tables_random_shapes_vs_oracle():
+    rng = np.random.default_rng(7)
+    for _ in range(20):
+        M = int(rng.integers(1, 24))
+        D = int(rng.integers(1, 6))
+        if S.hierarchy_size(M, D) > 300000:
+            continue
+        r1, e1 = capi.hierarchy_tables(M, D)
+        r2, e2 = O.hierarchy_tables(M, D)
+        np.testing.assert_array_equal(r1, r2)
+        np.testing.assert_array_equal(e1, e2)
+
+
+def _random_state(size, d, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((size, d, d)) + 1j * rng.standard_normal((size, d, d))
+    return x.astype(np.complex128)
+
+
+@pytest.mark.parametrize("n,K,depth", [(1, 1, 2), (2, 1, 3), (3, 2, 2), (4, 2, 2), (5, 1, 2), (6, 1, 1)])
+def test_rhs_matches_oracle(n, K, depth):
+    p = S.spin_glass(n, seed=100 + n, depth=depth, K=K, h=0.7)
+    o = O.Oracle(p)
+    with capi.Context(p) as ctx:
+        assert ctx.size == o.size
+        x = _random_state(ctx.size, p.dim, n)
+        ctx.set_state(x)
+        got = ctx.rhs()
+    want = o.rhs(x)
+    scale = max(1.0, np.max(np.abs(want)))
+    assert np.max(np.abs(got - want)) <= 1e-12 * scale
+    o.close()
+
+
+def test_rhs_general_diagonal_coupling():
+    """Non-Pauli diagonal V (counter term nonzero, both commutator and anti-commutator active)."""
+    p = S.spin_glass(3, seed=9, depth=2, K=2, h=0.3)
+    rng = np.random.default_rng(3)
+    for b in p.baths:
+        b.v_diag = rng.standard_normal(p.dim)
+    o = O.Oracle(p)
+    with capi.Context(p) as ctx:
+        x = _random_state(ctx.size, p.dim, 5)
+        ctx.set_state(x)
+        got = ctx.rhs()
+    want = o.rhs(x)
+    assert np.max(np.abs(got - want)) <= 1e-12 * max(1.0, np.max(np.abs(want)))
+    o.close()
+
+
+def test_c1_spin_glass_full_trajectory():
+    """The d=16, 12-mode, L=3 (455 ADO) spin glass: 1000 steps of rho_0(t), <H>(t)."""
+    p = S.spin_glass(4, seed=2024, depth=3, K=2, h=1.0, dt=0.01)
+    steps = 1000
+    o = O.Oracle(p)
+    rho_ref, en_ref = o.run(steps, trace=True)
+    with capi.Context(p) as ctx:
+        assert ctx.size == 455
+        rho, en = ctx.step_trace(steps)
+    assert np.max(np.abs(rho - rho_ref)) <= TOL
+    assert np.max(np.abs(en - en_ref)) <= TOL
+    # physical invariants of the reduced density
+    tr = np.trace(rho, axis1=1, axis2=2)
+    assert np.max(np.abs(tr - 1.0)) < 1e-10
+    assert np.max(np.abs(rho - np.conj(np.transpose(rho, (0, 2, 1))))) < 1e-10
+    o.close()
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 4, 6])
+def test_integration_orders(order):
+    p = S.spin_glass(3, seed=17, depth=3, K=1, h=0.9, dt=0.02)
+    o = O.Oracle(p)
+    rho_ref, en_ref = o.run(25, order=order, trace=True)
+    with capi.Context(p, order=order) as ctx:
+        rho, en = ctx.step_trace(25)
+    assert np.max(np.abs(rho - rho_ref)) <= TOL
+    assert np.max(np.abs(en - en_ref)) <= TOL
+    o.close()
+
+
+def test_d64_small_hierarchy_steps():
+    p = S.spin_glass(6, seed=77, depth=2, K=2, h=1.0, dt=0.005)
+    o = O.Oracle(p)
+    rho_ref, en_ref = o.run(20, trace=True)
+    with capi.Context(p) as ctx:
+        rho, en = ctx.step_trace(20)
+        ctx.step(5)
+        ctx.sync()
+        st = ctx.state()
+    o.run(5)
+    assert np.max(np.abs(rho - rho_ref)) <= TOL
+    assert np.max(np.abs(en - en_ref)) <= TOL
+    assert np.max(np.abs(st - o.state())) <= TOL
+    o.close()
+
+
+def test_c2_full_size_one_step_and_invariants():
+    """The d=64, 18-mode, L=4 (7315 ADO) FP64 workload: one step against the
+    oracle, then size-independent invariants over further steps."""
+    p = S.spin_glass(6, seed=2025, depth=4, K=2, h=1.0, dt=0.005)
+    with capi.Context(p) as ctx:
+        assert ctx.size == 7315
+        # populate every tier: start from a random Hermitian-ish state
+        x = _random_state(ctx.size, p.dim, 1) * 1e-3
+        x[0] = S.initial_rho0(p.dim)
+        ctx.set_state(x)
+        ctx.step(1)
+        ctx.sync()
+        got = ctx.state()
+        o = O.Oracle(p)
+        o.set_state(x)
+        o.run(1)
+        want = o.state()
+        o.close()
+        assert np.max(np.abs(got - want)) <= TOL
+        # invariants from the reference initial state
+        ctx.set_state(np.concatenate([S.initial_rho0(p.dim)[None], np.zeros((ctx.size - 1, 64, 64))]))
+        rho, en = ctx.step_trace(50)
+        tr = np.trace(rho, axis1=1, axis2=2)
+        assert np.max(np.abs(tr - 1.0)) < 1e-12
+        assert np.max(np.abs(rho - np.conj(np.transpose(rho, (0, 2, 1))))) < 1e-12
+        ctx.check_finite()
+
+
+def test_trace_mode_matches_stepwise_observables():
+    p = S.spin_glass(4, seed=5, depth=2, K=1, dt=0.01)
+    with capi.Context(p) as a, capi.Context(p) as b:
+        _, en = a.step_trace(6)
+        vals = []
+        for _ in range(6):
+            b.step(1)
+            e, tr = b.observables()
+            vals.append(e)
+            assert abs(tr - 1.0) < 1e-12
+        assert np.max(np.abs(en - np.array(vals))) == 0.0
+        np.testing.assert_array_equal(a.rho0(), b.rho0())
+
+
+def test_state_roundtrip_and_counters():
+    p = S.spin_glass(3, seed=1, depth=3, K=1)
+    with capi.Context(p) as ctx:
+        x = _random_state(ctx.size, p.dim, 2)
+        ctx.set_state(x)
+        np.testing.assert_array_equal(ctx.state(), x)
+        c0 = ctx.counters().stage_launches
+        ctx.step(3)
+        ctx.sync()
+        assert ctx.counters().stage_launches - c0 == 3 * 4
+        info = ctx.get_info()
+        assert info.steps_done == 3 and info.kernels_per_step == 4
+
+
+def test_initial_state_and_energy():
+    p = S.spin_glass(4, seed=2024, depth=3, K=2)
+    with capi.Context(p) as ctx:
+        e, tr = ctx.observables()
+        assert tr == 1.0
+        assert abs(e - p.h_diag[-1]) < 1e-14
+        np.testing.assert_array_equal(ctx.rho0(), S.initial_rho0(p.dim))
+
+
+def test_non_finite_state_is_reported():
+    p = S.spin_glass(2, seed=1, depth=2, K=1)
+    with capi.Context(p) as ctx:
+        x = np.zeros((ctx.size, p.dim, p.dim), np.complex128)
+        x[1, 0, 1] = np.nan
+        ctx.set_state(x)
+        with pytest.raises(capi.HxError) as err:
+            ctx.check_finite()
+        assert err.value.status == "NonFiniteState"
