@@ -27,7 +27,7 @@ PRECISION_DOUBLE = 1
 
 # Every exported symbol of include/helix_b200.h
 EXPORTS = [
-    "hx_last_error", "hx_version", "hx_hierarchy_size", "hx_hierarchy_tables", "hx_psd",
+    "hx_last_error", "hx_version", "hx_select_device", "hx_hierarchy_size", "hx_hierarchy_tables", "hx_psd",
     "hx_seeded_couplings", "hx_ctx_create", "hx_ctx_destroy", "hx_ctx_set_stream", "hx_ctx_get_stream",
     "hx_ctx_info", "hx_ctx_counters", "hx_ctx_step", "hx_ctx_step_trace", "hx_ctx_sync",
     "hx_ctx_read_rho0", "hx_ctx_observables", "hx_ctx_read_state", "hx_ctx_write_state",
@@ -87,6 +87,7 @@ def lib():
             vp, u32, u64, dp = C.c_void_p, C.c_uint32, C.c_uint64, C.POINTER(C.c_double)
             L.hx_last_error.restype = C.c_char_p
             L.hx_version.restype = C.c_char_p
+            L.hx_select_device.argtypes = [C.c_int]
             L.hx_hierarchy_size.argtypes = [u32, u32, C.POINTER(u64)]
             L.hx_hierarchy_tables.argtypes = [u32, u32, vp, vp, u64]
             L.hx_psd.argtypes = [u32, vp, vp]

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -49,7 +50,8 @@ void release(hx_ctx* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->rho, c->ua, c->ub, c->rows, c->edges, c->acoef, c->bcoef, c->gsum, c->hdiag,
                     c->hflip, c->vdiag, c->xi, c->counter, c->bath_off, c->error_flag, c->obs,
-                    c->trace_buf, c->energy_buf};
+                    c->trace_buf, c->energy_buf, c->diag_table, c->ent_count, c->ent_slab, c->ent_bath,
+                    c->ent_wc, c->ent_wa, c->order_perm};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -79,13 +81,41 @@ hx::StageTables tables_of(const hx_ctx* c)
     return t;
 }
 
+hx::Stage2Args stage2_args_of(const hx_ctx* c)
+{
+    hx::Stage2Args a{};
+    a.diag = c->diag_table;
+    a.vdiag = c->vdiag;
+    a.hflip = c->hflip;
+    a.gsum = c->gsum;
+    a.ent_count = c->ent_count;
+    a.ent_slab = c->ent_slab;
+    a.ent_bath = c->ent_bath;
+    a.ent_wc = c->ent_wc;
+    a.ent_wa = c->ent_wa;
+    a.order = c->order_perm;
+    a.error_flag = c->error_flag;
+    a.H = c->H;
+    a.M = c->M;
+    a.J = c->J;
+    a.logd = c->logd;
+    a.ctas = c->sm_count;
+    return a;
+}
+
+// One stage launch: the persistent kernel for d = 32, 64, the generic one otherwise.
+void launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
+{
+    if (c->use_stage2 && hx::launch_stage2(stage2_args_of(c), u, rho, out, alpha, base, c->stream)) return;
+    hx::launch_stage(tables_of(c), u, rho, out, alpha, base, c->stream);
+}
+
 // Enqueue one integrator step (Horner form of the order-m Taylor polynomial).
 int enqueue_step(hx_ctx* c)
 {
-    const hx::StageTables t = tables_of(c);
     const int m = c->order;
     if (m == 1) {
-        hx::launch_stage(t, c->rho, c->rho, c->ua, c->dt, hx::kBaseSelf, c->stream);
+        launch_stage_any(c, c->rho, c->rho, c->ua, c->dt, hx::kBaseSelf);
         std::swap(c->rho, c->ua);
     } else {
         const double2* in = c->rho;
@@ -93,7 +123,7 @@ int enqueue_step(hx_ctx* c)
         for (int s = 1; s <= m; ++s) {
             const double alpha = c->dt / static_cast<double>(m - s + 1);
             double2* out = (s == m) ? c->rho : bufs[(s - 1) & 1];
-            hx::launch_stage(t, in, c->rho, out, alpha, s == 1 ? hx::kBaseSelf : hx::kBaseRho, c->stream);
+            launch_stage_any(c, in, c->rho, out, alpha, s == 1 ? hx::kBaseSelf : hx::kBaseRho);
             in = out;
         }
     }
@@ -125,6 +155,13 @@ int read_error_flag(hx_ctx* c)
 }  // namespace
 
 extern "C" {
+
+int hx_select_device(int device)
+{
+    if (device < 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "CUDA device index must be non-negative");
+    HX_CUDA_TRY(cudaSetDevice(device));
+    return HX_OK;
+}
 
 int hx_hierarchy_tables(uint32_t modes, uint32_t max_depth, int32_t* rows, int32_t* edges, uint64_t count)
 {
@@ -291,6 +328,21 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                                 c->bcoef, c->gsum, c->stream);
         hx::launch_init_state(c->rho, static_cast<long long>(nstate), c->d, c->stream);
         rc = check_launch("setup kernels");
+    }
+    // persistent stage kernel (d = 32, 64): neighbour entry lists and the diagonal table
+    const char* force_generic = std::getenv("HX_FORCE_GENERIC_STAGE");
+    if (rc == HX_OK && logd >= 5 && hx::stage2_supported(logd, M, J) && !(force_generic && force_generic[0] == '1')) {
+        cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+        if ((rc = dev_alloc(c, &c->diag_table, c->slab)) || (rc = dev_alloc(c, &c->ent_count, H)) ||
+            (rc = dev_alloc(c, &c->ent_slab, H * 2 * M)) || (rc = dev_alloc(c, &c->ent_bath, H * 2 * M)) ||
+            (rc = dev_alloc(c, &c->ent_wc, H * 2 * M)) || (rc = dev_alloc(c, &c->ent_wa, H * 2 * M))) {
+        } else {
+            hx::launch_diag_table(c->hdiag, c->vdiag, c->xi, c->counter, c->d, J, c->diag_table, c->stream);
+            hx::launch_entries(c->edges, c->acoef, c->bcoef, c->bath_off, c->H, M, J, c->ent_count, c->ent_slab,
+                               c->ent_bath, c->ent_wc, c->ent_wa, c->stream);
+            rc = check_launch("stage-2 setup kernels");
+            c->use_stage2 = (rc == HX_OK) && c->sm_count > 0;
+        }
     }
     if (rc == HX_OK) {
         e = cudaStreamSynchronize(c->stream);
@@ -472,7 +524,7 @@ int hx_ctx_rhs(hx_ctx* c, double* out, uint64_t n)
     if (!c || !out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
     const size_t count = static_cast<size_t>(c->H) * c->slab;
     if (n < 2 * count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "output buffer too small");
-    hx::launch_stage(tables_of(c), c->rho, c->rho, c->ua, 1.0, hx::kBaseZero, c->stream);
+    launch_stage_any(c, c->rho, c->rho, c->ua, 1.0, hx::kBaseZero);
     c->counters.kernel_launches += 1;
     int rc = check_launch("stage kernel launch");
     if (rc != HX_OK) return rc;

@@ -79,6 +79,31 @@ enum BaseKind : int { kBaseSelf = 0, kBaseRho = 1, kBaseZero = 2 };
 void launch_stage(const StageTables& t, const double2* u, const double2* rho, double2* out,
                   double alpha, int base_kind, cudaStream_t s);
 
+// Persistent stage kernel for d = 32, 64 (hx_stage2.cu)
+struct Stage2Args {
+    const double2* diag;     // [d*d] ADO-independent diagonal coefficient table
+    const double* vdiag;     // [J][d]
+    const double* hflip;     // [log2 d]
+    const double* gsum;      // [H]
+    const int* ent_count;    // [H]
+    const int32_t* ent_slab; // [H][2M] neighbour slab
+    const int32_t* ent_bath; // [H][2M]
+    const double* ent_wc;    // [H][2M] commutator weight
+    const double* ent_wa;    // [H][2M] anti-commutator weight
+    const int32_t* order;    // [H] or nullptr
+    int* error_flag;
+    long long H;
+    int M, J, logd, ctas;
+};
+bool stage2_supported(int logd, int M, int J);
+bool launch_stage2(const Stage2Args& a, const double2* u, const double2* rho, double2* out, double alpha,
+                   int base_kind, cudaStream_t s);
+void launch_entries(const int32_t* edges, const double* acoef, const double* bcoef, const int32_t* bath_off,
+                    long long H, int M, int J, int* count, int32_t* slab, int32_t* bath, double* wc, double* wa,
+                    cudaStream_t s);
+void launch_diag_table(const double* hdiag, const double* vdiag, const double* xi, const double* kappa, int D, int J,
+                       double2* T, cudaStream_t s);
+
 // Tables on the device (hx_tables.cu)
 int build_tables_device(int M, int D, long long H, int32_t* d_rows, int32_t* d_edges, cudaStream_t s);
 void launch_coefficients(const int32_t* rows, long long H, int M, int J, const int32_t* mode_bath,
@@ -121,6 +146,16 @@ struct hx_ctx {
     double* counter = nullptr;
     int32_t* bath_off = nullptr;
     int* error_flag = nullptr;
+    // persistent stage-kernel tables (d = 32, 64)
+    bool use_stage2 = false;
+    int sm_count = 0;
+    double2* diag_table = nullptr;
+    int* ent_count = nullptr;
+    int32_t* ent_slab = nullptr;
+    int32_t* ent_bath = nullptr;
+    double* ent_wc = nullptr;
+    double* ent_wa = nullptr;
+    int32_t* order_perm = nullptr;
     double* obs = nullptr;        // [3] observables scratch
     double2* trace_buf = nullptr; // per-step rho_0 chunk
     double* energy_buf = nullptr;

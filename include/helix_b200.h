@@ -101,6 +101,11 @@ const char* hx_last_error(void);
 /* Library version string. (helix::runtimeVersion, src/helix.cpp:18-21) */
 const char* hx_version(void);
 
+/* Make `device` the calling thread's current CUDA device (contexts are
+ * created on the current device).  (cudaSetDevice in Context::Impl,
+ * src/helix.cpp:568-573) */
+int hx_select_device(int device);
+
 /* Number of ADOs for `modes` modes and exclusive depth bound `max_depth`.
  * (hierarchySizeFor, src/initialize_detail.h:159-172) */
 int hx_hierarchy_size(uint32_t modes, uint32_t max_depth, uint64_t* count);

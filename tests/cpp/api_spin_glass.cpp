@@ -1,0 +1,57 @@
+// Drives the helix:: C++ API the way a reference user does
+// (helix::HEOMSolver(options).run(system, hierarchy, solverOptions)) and
+// prints the result as JSON for tests/test_cpp_api.py to check against the
+// FP64 oracle.  Usage: api_spin_glass <spins> <seed> <h> <depth> <K> <steps> <dt> <mode>
+//   mode: final | trace | trajectory | legacy | sparse-bad
+#include <helix/helix.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+int main(int argc, char** argv)
+{
+    if (argc < 9) return 2;
+    const std::size_t spins = std::strtoul(argv[1], nullptr, 10);
+    const std::uint64_t seed = std::strtoull(argv[2], nullptr, 10);
+    const double h = std::atof(argv[3]);
+    const std::size_t depth = std::strtoul(argv[4], nullptr, 10);
+    const std::size_t K = std::strtoul(argv[5], nullptr, 10);
+    const std::size_t steps = std::strtoul(argv[6], nullptr, 10);
+    const double dt = std::atof(argv[7]);
+    const std::string mode = argv[8];
+
+    helix::ContextOptions options;
+    options.precision = helix::Precision::Double;
+    helix::System system = helix::examples::transverse_ising_spin_glass(spins, seed, h);
+    helix::HierarchySpec hierarchy = helix::examples::spin_glass_hierarchy(spins, 0.1, 1.0, 1.0, K, depth);
+    helix::SolverOptions solver;
+    solver.steps = steps;
+    solver.timeStep = dt;
+    if (mode == "trace") solver.resultMode = helix::ResultMode::ObservableTrace;
+    if (mode == "trajectory") solver.resultMode = helix::ResultMode::Trajectory;
+    if (mode == "legacy") system = helix::examples::legacy_spin_glass_system();
+    if (mode == "sparse-bad") {
+        // a column index outside the operator: System::from_sparse validation must flag it
+        helix::SparseOperator bad = system.couplings[0];
+        bad.columnIndices[0] = 1u << 20;
+        system = helix::System::from_sparse(system.hamiltonian, {bad});
+    }
+
+    const helix::RunResult result = helix::HEOMSolver(options).run(system, hierarchy, solver);
+    std::printf("{\"ok\": %s, \"codes\": [", result.ok() ? "true" : "false");
+    for (std::size_t i = 0; i < result.diagnostics.entries().size(); ++i)
+        std::printf("%s%d", i ? ", " : "", static_cast<int>(result.diagnostics.entries()[i].code));
+    std::printf("], \"hierarchy\": %zu, \"count\": %zu, \"rows\": %zu, \"times\": [",
+                result.diagnostics.hierarchySize, result.reduced_density_shape.count,
+                result.reduced_density_shape.rows);
+    for (std::size_t i = 0; i < result.times.size(); ++i) std::printf("%s%.17g", i ? ", " : "", result.times[i]);
+    std::printf("], \"energies\": [");
+    for (std::size_t i = 0; i < result.energies.size(); ++i) std::printf("%s%.17g", i ? ", " : "", result.energies[i]);
+    std::printf("], \"rho\": [");
+    for (std::size_t i = 0; i < result.reduced_density.size(); ++i)
+        std::printf("%s%.17g, %.17g", i ? ", " : "", result.reduced_density[i].real(), result.reduced_density[i].imag());
+    std::printf("], \"warnings\": %zu}\n", result.diagnostics.warnings.size());
+    return 0;
+}

@@ -1,0 +1,64 @@
+"""The helix:: C++ API (include/helix/*.h, libhelix.so) driven like the
+reference's public solver tests (tests/numerical/public_solver_spin_glass_tests.cu,
+public_result_shape_tests.cu): build a small program against the headers,
+run it, and check RunResult against the FP64 oracle."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helix_b200 import build as hb
+from helix_b200 import systems as S
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(hb.OUT, "api_spin_glass")
+
+
+@pytest.fixture(scope="module")
+def exe():
+    src = os.path.join(ROOT, "tests", "cpp", "api_spin_glass.cpp")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), src, "-L", hb.OUT,
+                    "-lhelix", "-lhelix_b200", f"-Wl,-rpath,{hb.OUT}", "-o", EXE], check=True)
+    return EXE
+
+
+def _run(exe, *args):
+    out = subprocess.run([exe, *map(str, args)], capture_output=True, text=True, check=True)
+    return json.loads(out.stdout)
+
+
+def test_cpp_api_compiles_and_validates_without_device(exe):
+    # the legacy adapter and broken CSR input are rejected during validation
+    r = _run(exe, 3, 1, 1.0, 2, 1, 1, 0.01, "legacy")
+    assert r["ok"] is False and 9 in r["codes"]          # UnsupportedExecution
+    r = _run(exe, 3, 1, 1.0, 2, 1, 1, 0.01, "sparse-bad")
+    assert r["ok"] is False and 3 in r["codes"]          # InvalidColumnIndex
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["final", "trace", "trajectory"])
+def test_cpp_api_matches_oracle(exe, mode):
+    spins, seed, h, depth, K, steps, dt = 4, 2024, 1.0, 2, 2, 30, 0.01
+    r = _run(exe, spins, seed, h, depth, K, steps, dt, mode)
+    assert r["ok"], r["codes"]
+    p = S.spin_glass(spins, seed=seed, depth=depth, K=K, h=h, dt=dt)
+    o = O.Oracle(p)
+    rho_ref, en_ref = o.run(steps, trace=True)
+    o.close()
+    d = p.dim
+    assert r["hierarchy"] == p.hierarchy_size() and r["rows"] == d
+    rho = np.array(r["rho"]).view(np.complex128).reshape(-1, d, d)
+    if mode == "trajectory":
+        assert r["count"] == steps and len(r["times"]) == steps
+        assert np.max(np.abs(rho - rho_ref)) <= 1e-10
+    else:
+        assert r["count"] == 1
+        assert np.max(np.abs(rho[0] - rho_ref[-1])) <= 1e-10
+    if mode == "final":
+        assert r["times"] == [pytest.approx(steps * dt, rel=0, abs=1e-15)]
+        assert abs(r["energies"][0] - en_ref[-1]) <= 1e-10
+    else:
+        assert np.max(np.abs(np.array(r["energies"]) - en_ref)) <= 1e-10

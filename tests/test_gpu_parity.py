@@ -205,3 +205,29 @@ def test_non_finite_state_is_reported():
         with pytest.raises(capi.HxError) as err:
             ctx.check_finite()
         assert err.value.status == "NonFiniteState"
+
+
+@pytest.mark.parametrize("generic", [False, True])
+@pytest.mark.parametrize("n,K,depth", [(5, 2, 2), (6, 2, 2), (6, 1, 3)])
+def test_both_stage_kernels_match_oracle(monkeypatch, generic, n, K, depth):
+    """d = 32 / 64 run on the persistent kernel by default; HX_FORCE_GENERIC_STAGE=1
+    selects the one-CTA-per-ADO kernel.  Both must match the oracle."""
+    if generic:
+        monkeypatch.setenv("HX_FORCE_GENERIC_STAGE", "1")
+    else:
+        monkeypatch.delenv("HX_FORCE_GENERIC_STAGE", raising=False)
+    p = S.spin_glass(n, seed=300 + n, depth=depth, K=K, h=0.8, dt=0.005)
+    o = O.Oracle(p)
+    with capi.Context(p) as ctx:
+        x = _random_state(ctx.size, p.dim, 11) * 1e-2
+        x[0] = S.initial_rho0(p.dim)
+        ctx.set_state(x)
+        got = ctx.rhs()
+        o.set_state(x)
+        want = o.rhs(x)
+        assert np.max(np.abs(got - want)) <= 1e-12 * max(1.0, np.max(np.abs(want)))
+        ctx.step(3)
+        ctx.sync()
+        o.run(3)
+        assert np.max(np.abs(ctx.state() - o.state())) <= TOL
+    o.close()
