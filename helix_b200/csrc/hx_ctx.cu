@@ -51,7 +51,8 @@ void release(hx_ctx* c)
     void* ptrs[] = {c->rho, c->ua, c->ub, c->rows, c->edges, c->acoef, c->bcoef, c->gsum, c->hdiag,
                     c->hflip, c->vdiag, c->xi, c->counter, c->bath_off, c->error_flag, c->obs,
                     c->trace_buf, c->energy_buf, c->diag_table, c->ent_count, c->ent_slab, c->ent_bath,
-                    c->ent_wc, c->ent_wa, c->order_perm};
+                    c->ent_wc, c->ent_wa, c->order_perm, c->ado_keep, c->up_slot, c->up_ado, c->up_cnt,
+                    c->up_slab, c->up_bath, c->U};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -81,9 +82,9 @@ hx::StageTables tables_of(const hx_ctx* c)
     return t;
 }
 
-hx::Stage2Args stage2_args_of(const hx_ctx* c)
+hx::FusedArgs fused_args_of(const hx_ctx* c)
 {
-    hx::Stage2Args a{};
+    hx::FusedArgs a{};
     a.diag = c->diag_table;
     a.vdiag = c->vdiag;
     a.hflip = c->hflip;
@@ -94,28 +95,41 @@ hx::Stage2Args stage2_args_of(const hx_ctx* c)
     a.ent_wc = c->ent_wc;
     a.ent_wa = c->ent_wa;
     a.order = c->order_perm;
+    a.ado_keep = c->ado_keep;
+    a.slot = c->up_slot;
+    a.U = c->U;
     a.error_flag = c->error_flag;
     a.H = c->H;
     a.M = c->M;
     a.J = c->J;
     a.logd = c->logd;
-    a.ctas = c->sm_count;
     return a;
 }
 
-// One stage launch: the persistent kernel for d = 32, 64, the generic one otherwise.
-void launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
+// One stage: for d = 32, 64 the up-term kernel of tier L-1 followed by the
+// fused multi-CTA kernel; the generic kernel otherwise.  Returns kernels launched.
+int launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
 {
-    if (c->use_stage2 && hx::launch_stage2(stage2_args_of(c), u, rho, out, alpha, base, c->stream)) return;
+    if (c->use_fused) {
+        int k = 0;
+        if (c->up_slots > 0) {
+            hx::UpTermArgs ua{c->vdiag, c->up_cnt, c->up_slab, c->up_bath, c->bath_off, c->up_slots, c->M, c->J, c->logd};
+            hx::launch_upterm(ua, u, c->U, c->stream);
+            ++k;
+        }
+        if (hx::launch_fused(fused_args_of(c), u, rho, out, alpha, base, c->stream)) return k + 1;
+    }
     hx::launch_stage(tables_of(c), u, rho, out, alpha, base, c->stream);
+    return 1;
 }
 
 // Enqueue one integrator step (Horner form of the order-m Taylor polynomial).
 int enqueue_step(hx_ctx* c)
 {
     const int m = c->order;
+    int launched = 0;
     if (m == 1) {
-        launch_stage_any(c, c->rho, c->rho, c->ua, c->dt, hx::kBaseSelf);
+        launched += launch_stage_any(c, c->rho, c->rho, c->ua, c->dt, hx::kBaseSelf);
         std::swap(c->rho, c->ua);
     } else {
         const double2* in = c->rho;
@@ -123,11 +137,11 @@ int enqueue_step(hx_ctx* c)
         for (int s = 1; s <= m; ++s) {
             const double alpha = c->dt / static_cast<double>(m - s + 1);
             double2* out = (s == m) ? c->rho : bufs[(s - 1) & 1];
-            launch_stage_any(c, in, c->rho, out, alpha, s == 1 ? hx::kBaseSelf : hx::kBaseRho);
+            launched += launch_stage_any(c, in, c->rho, out, alpha, s == 1 ? hx::kBaseSelf : hx::kBaseRho);
             in = out;
         }
     }
-    c->counters.kernel_launches += m;
+    c->counters.kernel_launches += launched;
     c->counters.stage_launches += m;
     c->steps_done += 1;
     return HX_OK;
@@ -329,24 +343,59 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
         hx::launch_init_state(c->rho, static_cast<long long>(nstate), c->d, c->stream);
         rc = check_launch("setup kernels");
     }
-    // persistent stage kernel (d = 32, 64): neighbour entry lists and the diagonal table
+    // fused stage kernel (d = 32, 64): neighbour entry lists, diagonal table, up-term tables
     const char* force_generic = std::getenv("HX_FORCE_GENERIC_STAGE");
-    if (rc == HX_OK && logd >= 5 && hx::stage2_supported(logd, M, J) && !(force_generic && force_generic[0] == '1')) {
+    if (rc == HX_OK && logd >= 5 && hx::fused_supported(logd, M, J) && !(force_generic && force_generic[0] == '1')) {
         cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+        int* dS = nullptr;
         if ((rc = dev_alloc(c, &c->diag_table, c->slab)) || (rc = dev_alloc(c, &c->ent_count, H)) ||
             (rc = dev_alloc(c, &c->ent_slab, H * 2 * M)) || (rc = dev_alloc(c, &c->ent_bath, H * 2 * M)) ||
-            (rc = dev_alloc(c, &c->ent_wc, H * 2 * M)) || (rc = dev_alloc(c, &c->ent_wa, H * 2 * M))) {
+            (rc = dev_alloc(c, &c->ent_wc, H * 2 * M)) || (rc = dev_alloc(c, &c->ent_wa, H * 2 * M)) ||
+            (rc = dev_alloc(c, &c->ado_keep, H)) || (rc = dev_alloc(c, &c->up_slot, H)) ||
+            (rc = dev_alloc(c, &c->up_ado, H)) || (rc = dev_alloc(c, &c->up_cnt, H)) || (rc = dev_alloc(c, &dS, 1))) {
         } else {
             hx::launch_diag_table(c->hdiag, c->vdiag, c->xi, c->counter, c->d, J, c->diag_table, c->stream);
-            hx::launch_entries(c->edges, c->acoef, c->bcoef, c->bath_off, c->H, M, J, c->ent_count, c->ent_slab,
-                               c->ent_bath, c->ent_wc, c->ent_wa, c->stream);
-            rc = check_launch("stage-2 setup kernels");
-            c->use_stage2 = (rc == HX_OK) && c->sm_count > 0;
+            hx::launch_entries(c->rows, c->edges, c->acoef, c->bcoef, c->bath_off, c->H, M, J,
+                               static_cast<int>(p->max_depth), c->ent_count, c->ent_slab, c->ent_bath, c->ent_wc,
+                               c->ent_wa, c->ado_keep, c->stream);
+            rc = check_launch("fused-kernel setup");
+            // tier L-1 slots: count them first, then size the per-slot tables and U
+            int S = 0;
+            if (rc == HX_OK && p->max_depth >= 2) {
+                int32_t *tmp_slab = nullptr, *tmp_bath = nullptr;
+                e = cudaMalloc(&tmp_slab, H * M * sizeof(int32_t));
+                if (e == cudaSuccess) e = cudaMalloc(&tmp_bath, H * M * sizeof(int32_t));
+                if (e == cudaSuccess) {
+                    hx::launch_upterm_tables(c->rows, c->edges, dmb, c->H, M, static_cast<int>(p->max_depth) - 1,
+                                             c->up_slot, dS, c->up_ado, c->up_cnt, tmp_slab, tmp_bath, c->stream);
+                    e = cudaMemcpyAsync(&S, dS, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+                }
+                if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+                if (e == cudaSuccess && S > 0) {
+                    rc = dev_alloc(c, &c->up_slab, static_cast<size_t>(S) * M);
+                    if (rc == HX_OK) rc = dev_alloc(c, &c->up_bath, static_cast<size_t>(S) * M);
+                    if (rc == HX_OK) rc = dev_alloc(c, &c->U, static_cast<size_t>(S) * c->slab);
+                    if (rc == HX_OK) {
+                        e = cudaMemcpyAsync(c->up_slab, tmp_slab, static_cast<size_t>(S) * M * sizeof(int32_t),
+                                            cudaMemcpyDeviceToDevice, c->stream);
+                        if (e == cudaSuccess)
+                            e = cudaMemcpyAsync(c->up_bath, tmp_bath, static_cast<size_t>(S) * M * sizeof(int32_t),
+                                                cudaMemcpyDeviceToDevice, c->stream);
+                        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+                    }
+                }
+                if (e != cudaSuccess && rc == HX_OK) rc = hx::cuda_fail(e, "up-term tables");
+                cudaFree(tmp_slab);
+                cudaFree(tmp_bath);
+            } else if (rc == HX_OK) {
+                e = cudaMemsetAsync(c->up_slot, 0xff, H * sizeof(int32_t), c->stream);
+                if (e != cudaSuccess) rc = hx::cuda_fail(e, "up-term tables");
+            }
+            c->up_slots = S;
+            c->use_fused = (rc == HX_OK);
         }
-    }
-    if (rc == HX_OK) {
-        e = cudaStreamSynchronize(c->stream);
-        if (e != cudaSuccess) rc = hx::cuda_fail(e, "context setup");
+        cudaFree(dS);
+        if (dS) c->device_bytes -= sizeof(int);
     }
     cudaFree(dmb);
     cudaFree(dmk);
@@ -524,8 +573,7 @@ int hx_ctx_rhs(hx_ctx* c, double* out, uint64_t n)
     if (!c || !out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
     const size_t count = static_cast<size_t>(c->H) * c->slab;
     if (n < 2 * count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "output buffer too small");
-    launch_stage_any(c, c->rho, c->rho, c->ua, 1.0, hx::kBaseZero);
-    c->counters.kernel_launches += 1;
+    c->counters.kernel_launches += launch_stage_any(c, c->rho, c->rho, c->ua, 1.0, hx::kBaseZero);
     int rc = check_launch("stage kernel launch");
     if (rc != HX_OK) return rc;
     HX_CUDA_TRY(cudaMemcpyAsync(out, c->ua, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));

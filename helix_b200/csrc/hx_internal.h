@@ -79,30 +79,47 @@ enum BaseKind : int { kBaseSelf = 0, kBaseRho = 1, kBaseZero = 2 };
 void launch_stage(const StageTables& t, const double2* u, const double2* rho, double2* out,
                   double alpha, int base_kind, cudaStream_t s);
 
-// Persistent stage kernel for d = 32, 64 (hx_stage2.cu)
-struct Stage2Args {
+// Fused multi-CTA stage kernel for d = 32, 64 (hx_fused.cu)
+struct FusedArgs {
     const double2* diag;     // [d*d] ADO-independent diagonal coefficient table
     const double* vdiag;     // [J][d]
     const double* hflip;     // [log2 d]
     const double* gsum;      // [H]
     const int* ent_count;    // [H]
     const int32_t* ent_slab; // [H][2M] neighbour slab
-    const int32_t* ent_bath; // [H][2M]
+    const int32_t* ent_bath; // [H][2M] bath | (keep-in-L2 flag << 16)
     const double* ent_wc;    // [H][2M] commutator weight
     const double* ent_wa;    // [H][2M] anti-commutator weight
     const int32_t* order;    // [H] or nullptr
+    const int8_t* ado_keep;  // [H] 1 = slab below the top tier (evict_last in L2)
+    const int32_t* slot;     // [H] slot of a tier L-1 ADO in U, else -1
+    const double2* U;        // [S][d*d] up terms of tier L-1 (hx_upterm.cu)
     int* error_flag;
     long long H;
-    int M, J, logd, ctas;
+    int M, J, logd;
 };
-bool stage2_supported(int logd, int M, int J);
-bool launch_stage2(const Stage2Args& a, const double2* u, const double2* rho, double2* out, double alpha,
-                   int base_kind, cudaStream_t s);
-void launch_entries(const int32_t* edges, const double* acoef, const double* bcoef, const int32_t* bath_off,
-                    long long H, int M, int J, int* count, int32_t* slab, int32_t* bath, double* wc, double* wa,
-                    cudaStream_t s);
+bool fused_supported(int logd, int M, int J);
+bool launch_fused(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
+                  int base_kind, cudaStream_t s);
+void launch_entries(const int32_t* rows, const int32_t* edges, const double* acoef, const double* bcoef,
+                    const int32_t* bath_off, long long H, int M, int J, int max_depth, int* count, int32_t* slab,
+                    int32_t* bath, double* wc, double* wa, int8_t* keep, cudaStream_t s);
 void launch_diag_table(const double* hdiag, const double* vdiag, const double* xi, const double* kappa, int D, int J,
                        double2* T, cudaStream_t s);
+
+// Up term of tier L-1, element-tiled (hx_upterm.cu)
+struct UpTermArgs {
+    const double* vdiag;    // [J][d]
+    const int* cnt;         // [S]
+    const int32_t* slab;    // [S][M] up neighbour per mode
+    const int32_t* bath;    // [S][M]
+    const int32_t* bath_off;// [J+1]
+    int S, M, J, logd;
+};
+void launch_upterm(const UpTermArgs& a, const double2* u, double2* U, cudaStream_t s);
+void launch_upterm_tables(const int32_t* rows, const int32_t* edges, const int32_t* mode_bath, long long H, int M,
+                          int top, int32_t* slot, int* S_out, int32_t* ado, int* cnt, int32_t* slab, int32_t* bath,
+                          cudaStream_t s);
 
 // Tables on the device (hx_tables.cu)
 int build_tables_device(int M, int D, long long H, int32_t* d_rows, int32_t* d_edges, cudaStream_t s);
@@ -146,9 +163,16 @@ struct hx_ctx {
     double* counter = nullptr;
     int32_t* bath_off = nullptr;
     int* error_flag = nullptr;
-    // persistent stage-kernel tables (d = 32, 64)
-    bool use_stage2 = false;
+    // fused stage-kernel tables (d = 32, 64)
+    bool use_fused = false;
     int sm_count = 0;
+    int up_slots = 0;             // ADOs in tier L-1
+    int32_t* up_slot = nullptr;   // [H]
+    int32_t* up_ado = nullptr;    // [S]
+    int* up_cnt = nullptr;        // [S]
+    int32_t* up_slab = nullptr;   // [S][M]
+    int32_t* up_bath = nullptr;   // [S][M]
+    double2* U = nullptr;         // [S][d*d]
     double2* diag_table = nullptr;
     int* ent_count = nullptr;
     int32_t* ent_slab = nullptr;
@@ -156,6 +180,7 @@ struct hx_ctx {
     double* ent_wc = nullptr;
     double* ent_wa = nullptr;
     int32_t* order_perm = nullptr;
+    int8_t* ado_keep = nullptr;
     double* obs = nullptr;        // [3] observables scratch
     double2* trace_buf = nullptr; // per-step rho_0 chunk
     double* energy_buf = nullptr;

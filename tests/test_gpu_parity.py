@@ -207,15 +207,16 @@ def test_non_finite_state_is_reported():
         assert err.value.status == "NonFiniteState"
 
 
-@pytest.mark.parametrize("generic", [False, True])
-@pytest.mark.parametrize("n,K,depth", [(5, 2, 2), (6, 2, 2), (6, 1, 3)])
-def test_both_stage_kernels_match_oracle(monkeypatch, generic, n, K, depth):
-    """d = 32 / 64 run on the persistent kernel by default; HX_FORCE_GENERIC_STAGE=1
-    selects the one-CTA-per-ADO kernel.  Both must match the oracle."""
-    if generic:
+@pytest.mark.parametrize("variant", ["generic", "fused"])
+@pytest.mark.parametrize("n,K,depth", [(5, 2, 2), (6, 2, 2), (6, 1, 3), (5, 1, 0), (6, 2, 1)])
+def test_all_stage_kernels_match_oracle(monkeypatch, variant, n, K, depth):
+    """d = 32 / 64 run the up-term kernel + fused multi-CTA kernel by default;
+    HX_FORCE_GENERIC_STAGE=1 selects the generic one-slab-per-CTA kernel.
+    Both must match the oracle, including depth 0 (no hierarchy) and depth 1
+    (every tier-0 up neighbour handled by the up-term kernel)."""
+    monkeypatch.delenv("HX_FORCE_GENERIC_STAGE", raising=False)
+    if variant == "generic":
         monkeypatch.setenv("HX_FORCE_GENERIC_STAGE", "1")
-    else:
-        monkeypatch.delenv("HX_FORCE_GENERIC_STAGE", raising=False)
     p = S.spin_glass(n, seed=300 + n, depth=depth, K=K, h=0.8, dt=0.005)
     o = O.Oracle(p)
     with capi.Context(p) as ctx:
