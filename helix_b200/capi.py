@@ -31,7 +31,7 @@ EXPORTS = [
     "hx_seeded_couplings", "hx_ctx_create", "hx_ctx_destroy", "hx_ctx_set_stream", "hx_ctx_get_stream",
     "hx_ctx_info", "hx_ctx_counters", "hx_ctx_step", "hx_ctx_step_trace", "hx_ctx_sync",
     "hx_ctx_read_rho0", "hx_ctx_observables", "hx_ctx_read_state", "hx_ctx_write_state",
-    "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_check_finite",
+    "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_check_finite", "hx_rhs_noalloc",
 ]
 
 
@@ -109,6 +109,7 @@ def lib():
             L.hx_ctx_state_device_ptr.argtypes = [vp, C.POINTER(vp)]
             L.hx_ctx_rhs.argtypes = [vp, vp, u64]
             L.hx_ctx_check_finite.argtypes = [vp]
+            L.hx_rhs_noalloc.argtypes = [C.POINTER(_Problem), vp, vp, vp]
             _lib = L
         return _lib
 
@@ -152,6 +153,37 @@ def seeded_couplings(n: int, seed: int) -> np.ndarray:
     J = np.zeros((n, n))
     _check(lib().hx_seeded_couplings(n, seed, _p(J)))
     return J
+
+
+def _problem_struct(problem, order: int = 4, dt: float | None = None):
+    """hx_problem for a systems.Problem; returns (struct, keep-alive list)."""
+    d = problem.dim
+    keep = []
+    hd = np.ascontiguousarray(problem.h_diag, np.float64)
+    hf = np.ascontiguousarray(problem.h_flip, np.float64)
+    keep += [hd, hf]
+    baths = (_Bath * len(problem.baths))()
+    for j, b in enumerate(problem.baths):
+        if b.v_diag is None:
+            raise HxError(11, "the fused path needs diagonal coupling operators")
+        v = np.ascontiguousarray(b.v_diag, np.float64)
+        if v.ndim != 1 or v.shape[0] < d:
+            raise HxError(5, "coupling operator dimensions must match the system operator")
+        keep.append(v)
+        baths[j] = _Bath(b.beta, b.gamma, b.zeta, b.K, v.ctypes.data_as(C.POINTER(C.c_double)))
+    keep.append(baths)
+    prob = _Problem(d, hd.ctypes.data_as(C.POINTER(C.c_double)), hf.ctypes.data_as(C.POINTER(C.c_double)),
+                    len(problem.baths), baths, problem.max_depth, problem.dt if dt is None else dt, order,
+                    PRECISION_DOUBLE, 0)
+    return prob, keep
+
+
+def rhs_noalloc(problem, rho_device_ptr: int, drho_device_ptr: int, stream_ptr: int | None = None) -> None:
+    """drho = L(rho) through hx_rhs_noalloc (device pointers; allocates nothing)."""
+    prob, keep = _problem_struct(problem)
+    _check(lib().hx_rhs_noalloc(C.byref(prob), C.c_void_p(rho_device_ptr), C.c_void_p(drho_device_ptr),
+                                C.c_void_p(stream_ptr or 0)))
+    del keep
 
 
 class Context:

@@ -123,6 +123,10 @@ void launch_upterm_tables(const int32_t* rows, const int32_t* edges, const int32
 
 // Tables on the device (hx_tables.cu)
 int build_tables_device(int M, int D, long long H, int32_t* d_rows, int32_t* d_edges, cudaStream_t s);
+// Same table kernel with a binomial table (rows n <= M + D, columns k <= M,
+// kcols = M + 1) that the caller already placed in device memory.
+void launch_tables_with_binomials(const unsigned long long* d_binom, int kcols, int M, int D, long long H,
+                                  int32_t* d_rows, int32_t* d_edges, cudaStream_t s);
 void launch_coefficients(const int32_t* rows, long long H, int M, int J, const int32_t* mode_bath,
                          const int32_t* mode_k, const double* nu, const double* theta_c,
                          const double* theta_a, const double* phi, const int32_t* bath_off,

@@ -145,6 +145,15 @@ int build_tables_device(int M, int D, long long H, int32_t* d_rows, int32_t* d_e
     return HX_OK;
 }
 
+void launch_tables_with_binomials(const unsigned long long* d_binom, int kcols, int M, int D, long long H,
+                                  int32_t* d_rows, int32_t* d_edges, cudaStream_t s)
+{
+    if (H <= 0) return;
+    const int block = 128;
+    const long long grid = (H + block - 1) / block;
+    tables_kernel<<<static_cast<unsigned>(grid), block, 0, s>>>(Binom{d_binom, kcols}, M, D, H, d_rows, d_edges);
+}
+
 void launch_coefficients(const int32_t* rows, long long H, int M, int J, const int32_t* mode_bath,
                          const int32_t* mode_k, const double* nu, const double* theta_c,
                          const double* theta_a, const double* phi, const int32_t* bath_off,
