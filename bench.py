@@ -56,7 +56,7 @@ def load_peaks() -> tuple[float, str]:
 
 def profiled_traffic(config: str) -> float | None:
     """DRAM bytes per stage launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", f"stage_kernel_{config}_ncu.txt")
+    path = os.path.join(ROOT, "profiles", f"fused_kernel_{config}_ncu.txt")
     try:
         with open(path) as f:
             for line in f:
@@ -268,7 +268,7 @@ def run_ours(args, cfg: dict) -> None:
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
                          "algorithmic_bytes_per_launch": per_launch_bytes,
-                         "kernel": "stage_kernel<6>", "launch_ms": launch_ms},
+                         "kernel": "fused_kernel<6,2> + upterm_kernel per stage", "launch_ms": launch_ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": p.dim * p.dim * 16 + 24,
                     "path": "hx_ctx_write_state (pinned host) + hx_ctx_step_trace (rho0, <H> per step) + hx_ctx_read_rho0"},
