@@ -37,10 +37,14 @@ CONFIGS = {
                workload="spin_glass_d64_L4_K2_7315ados_fp64"),
     "c1": dict(n=4, depth=3, K=2, h=1.0, dt=0.01, seed=2024,
                workload="spin_glass_d16_L3_K2_455ados_fp64"),
+    # the reference's compiled default: d=1024, one collective bath (3 modes), 10 ADOs, dt=0.1
+    "legacy": dict(legacy=True, dim=1024, workload="legacy_spin_glass_d1024_10ados_fp64"),
 }
 
 
 def make_problem(cfg: dict, rank: int = 0):
+    if cfg.get("legacy"):
+        return S.legacy_spin_glass(cfg["dim"])
     return S.spin_glass(cfg["n"], seed=cfg["seed"] + rank, depth=cfg["depth"], K=cfg["K"], h=cfg["h"],
                         dt=cfg["dt"])
 
@@ -259,7 +263,8 @@ def run_ours(args, cfg: dict) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "ados": H, "dim": p.dim, "modes": p.modes, "depth_L": cfg["depth"],
+            "config": {"workload": cfg["workload"], "ados": H, "dim": p.dim, "modes": p.modes,
+                       "depth_L": p.max_depth - 1,
                        "dt": p.dt, "integrator": "RK4 (4-term Taylor, Horner form)",
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": f"inputs larger than L2 (state {state_bytes / 1e9:.3f} GB)"},

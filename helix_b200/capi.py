@@ -45,7 +45,7 @@ class HxError(RuntimeError):
 class _Bath(C.Structure):
     _fields_ = [("inverse_temperature", C.c_double), ("damping", C.c_double),
                 ("coupling_strength", C.c_double), ("pade_terms", C.c_uint32),
-                ("coupling_diag", C.POINTER(C.c_double))]
+                ("coupling_diag", C.POINTER(C.c_double)), ("coupling_flip", C.POINTER(C.c_double))]
 
 
 class _Problem(C.Structure):
@@ -158,6 +158,7 @@ def seeded_couplings(n: int, seed: int) -> np.ndarray:
 def _problem_struct(problem, order: int = 4, dt: float | None = None):
     """hx_problem for a systems.Problem; returns (struct, keep-alive list)."""
     d = problem.dim
+    n = problem.n_spins
     keep = []
     hd = np.ascontiguousarray(problem.h_diag, np.float64)
     hf = np.ascontiguousarray(problem.h_flip, np.float64)
@@ -165,12 +166,19 @@ def _problem_struct(problem, order: int = 4, dt: float | None = None):
     baths = (_Bath * len(problem.baths))()
     for j, b in enumerate(problem.baths):
         if b.v_diag is None:
-            raise HxError(11, "the fused path needs diagonal coupling operators")
+            raise HxError(11, "coupling operators must be given as diagonal + per-spin flip weights")
         v = np.ascontiguousarray(b.v_diag, np.float64)
         if v.ndim != 1 or v.shape[0] < d:
             raise HxError(5, "coupling operator dimensions must match the system operator")
         keep.append(v)
-        baths[j] = _Bath(b.beta, b.gamma, b.zeta, b.K, v.ctypes.data_as(C.POINTER(C.c_double)))
+        fp = None
+        if b.v_flip is not None:
+            f = np.ascontiguousarray(b.v_flip, np.float64)
+            if f.shape != (n,):
+                raise HxError(5, "coupling flip weights need one value per spin")
+            keep.append(f)
+            fp = f.ctypes.data_as(C.POINTER(C.c_double))
+        baths[j] = _Bath(b.beta, b.gamma, b.zeta, b.K, v.ctypes.data_as(C.POINTER(C.c_double)), fp)
     keep.append(baths)
     prob = _Problem(d, hd.ctypes.data_as(C.POINTER(C.c_double)), hf.ctypes.data_as(C.POINTER(C.c_double)),
                     len(problem.baths), baths, problem.max_depth, problem.dt if dt is None else dt, order,
@@ -193,23 +201,7 @@ class Context:
         L = lib()
         self.problem = problem
         d = problem.dim
-        self._keep = []
-        hd = np.ascontiguousarray(problem.h_diag, np.float64)
-        hf = np.ascontiguousarray(problem.h_flip, np.float64)
-        self._keep += [hd, hf]
-        baths = (_Bath * len(problem.baths))()
-        for j, b in enumerate(problem.baths):
-            if b.v_diag is None:
-                raise HxError(11, "the fused path needs diagonal coupling operators")
-            v = np.ascontiguousarray(b.v_diag, np.float64)
-            if v.ndim != 1 or v.shape[0] < d:
-                raise HxError(5, "coupling operator dimensions must match the system operator")
-            self._keep.append(v)
-            baths[j] = _Bath(b.beta, b.gamma, b.zeta, b.K, v.ctypes.data_as(C.POINTER(C.c_double)))
-        self._keep.append(baths)
-        prob = _Problem(d, hd.ctypes.data_as(C.POINTER(C.c_double)), hf.ctypes.data_as(C.POINTER(C.c_double)),
-                        len(problem.baths), baths, problem.max_depth,
-                        problem.dt if dt is None else dt, order, PRECISION_DOUBLE, 0)
+        prob, self._keep = _problem_struct(problem, order, dt)
         h = C.c_void_p()
         _check(L.hx_ctx_create(C.byref(prob), C.byref(h)))
         self._h = h

@@ -140,12 +140,88 @@ Diagnostics validate_solver_options(const SolverOptions& o)
     return d;
 }
 
-// The executable structure: H = diag(E) + sum_i h_i sx_i (real), couplings diagonal (real).
+// The executable structure: H = diag(E) + sum_i h_i sx_i (real), each coupling
+// V_j = diag(v_j) + sum_i w_ji sx_i (real).
 struct Lowered {
     uint32_t dim = 0;
     std::vector<double> hdiag, hflip;
-    std::vector<std::vector<double>> vdiag;
+    std::vector<std::vector<double>> vdiag, vflip;
 };
+
+// Split a real CSR operator into its diagonal and per-spin flip weights;
+// false if it has any other structure.
+bool split_flip_operator(const SparseOperator& op, std::size_t d, int n, std::vector<double>& diag,
+                         std::vector<double>& flip, std::string& why, const char* name)
+{
+    diag.assign(d, 0.0);
+    flip.assign(n, 0.0);
+    std::vector<int> count(n, 0);
+    for (std::size_t r = 0; r < d; ++r)
+        for (std::size_t p = op.rowOffsets[r]; p < op.rowOffsets[r + 1]; ++p) {
+            const std::size_t c = op.columnIndices[p];
+            const std::complex<double> v = op.values[p];
+            if (v.imag() != 0.0) {
+                why = std::string(name) + ": complex entries are outside the supported structure";
+                return false;
+            }
+            if (c == r) {
+                diag[r] += v.real();
+                continue;
+            }
+            const std::size_t x = r ^ c;
+            if ((x & (x - 1)) != 0) {
+                why = std::string(name) + ": off-diagonal entries must be single-spin flips";
+                return false;
+            }
+            int bit = 0;
+            while ((std::size_t(1) << bit) != x) ++bit;
+            if (count[bit] > 0 && flip[bit] != v.real()) {
+                why = std::string(name) + ": the flip of one spin must carry one value";
+                return false;
+            }
+            flip[bit] = v.real();
+            ++count[bit];
+        }
+    for (int b = 0; b < n; ++b)
+        if (count[b] != 0 && static_cast<std::size_t>(count[b]) != d) {
+            why = std::string(name) + ": a spin flip must act on every basis state";
+            return false;
+        }
+    return true;
+}
+
+// The reference's compiled spin-glass model (src/parameters.cu:11-18,
+// src/initialize.cu:95-157, initialize_detail.h:38-157): d = 1024, diagonal H
+// from the nearest-neighbour chain (J = 0.6) with projections +-1/2, one
+// collective V = sum_i s_z(i) + sum_{i : 2^i in the sparse flip masks} sx(i)
+// (mask 512 is absent from those masks).
+Lowered legacy_model()
+{
+    const int n = 10;
+    const std::size_t d = std::size_t(1) << n;
+    Lowered L;
+    L.dim = static_cast<uint32_t>(d);
+    L.hdiag.assign(d, 0.0);
+    L.hflip.assign(n, 0.0);
+    std::vector<double> v(d, 0.0), w(n, 0.0);
+    for (std::size_t state = 0; state < d; ++state) {
+        double p[n];
+        double total = 0.0;
+        for (int s = 0; s < n; ++s) {
+            p[s] = ((state >> s) & 1) ? 0.5 : -0.5;
+            total += p[s];
+        }
+        v[state] = total;
+        for (int j = 0; j < n; ++j)
+            for (int k = 0; k < j; ++k)
+                if (j - k == 1) total += 0.6 * p[j] * p[k];
+        L.hdiag[state] = total;
+    }
+    for (int i = 0; i < n; ++i) w[i] = ((1 << i) <= 256) ? 1.0 : 0.0;
+    L.vdiag.push_back(v);
+    L.vflip.push_back(w);
+    return L;
+}
 
 bool lower_system(const System& s, Lowered& out, std::string& why)
 {
@@ -202,17 +278,13 @@ bool lower_system(const System& s, Lowered& out, std::string& why)
             }
         }
     out.vdiag.clear();
-    for (const auto& V : s.couplings) {
-        std::vector<double> v(d, 0.0);
-        for (std::size_t r = 0; r < d; ++r)
-            for (std::size_t p = V.rowOffsets[r]; p < V.rowOffsets[r + 1]; ++p) {
-                if (V.columnIndices[p] != r || V.values[p].imag() != 0.0) {
-                    why = "coupling operators must be real diagonal for the fused path";
-                    return false;
-                }
-                v[r] += V.values[p].real();
-            }
+    out.vflip.clear();
+    for (std::size_t k = 0; k < s.couplings.size(); ++k) {
+        std::vector<double> v, w;
+        const std::string name = "coupling[" + std::to_string(k) + "]";
+        if (!split_flip_operator(s.couplings[k], d, n, v, w, why, name.c_str())) return false;
         out.vdiag.push_back(std::move(v));
+        out.vflip.push_back(std::move(w));
     }
     if (out.vdiag.empty()) {
         why = "at least one coupling operator is required";
@@ -377,6 +449,7 @@ public:
             baths[j].coupling_strength = b.couplingStrength;
             baths[j].pade_terms = static_cast<uint32_t>(b.padeTerms);
             baths[j].coupling_diag = sys.vdiag[j].data();
+            baths[j].coupling_flip = sys.vflip.size() > j ? sys.vflip[j].data() : nullptr;
         }
         hx_problem p{};
         p.dim = sys.dim;
@@ -526,9 +599,8 @@ Diagnostics validate_problem(const System& system, const HierarchySpec& hierarch
     append(d, hierarchy.validate_supported());
     append(d, validate_solver_options(options));
     if (system.kind == SystemKind::LegacySpinGlass) {
-        d.add(StatusCode::UnsupportedExecution,
-              "the legacy spin-glass adapter (non-diagonal collective coupling) is not executed by the fused "
-              "path; use System::from_sparse with diagonal couplings");
+        if (hierarchy.baths.size() > 1)
+            d.add(StatusCode::UnsupportedHierarchy, "the legacy spin-glass model has one collective bath");
     } else if (system.kind == SystemKind::Dense) {
         d.add(StatusCode::UnsupportedSystemKind, "dense systems are not executed; use System::from_sparse");
     } else if (d.ok()) {
@@ -559,7 +631,9 @@ RunResult HEOMSolver::run_steps(std::size_t steps)
     try {
         Lowered low;
         std::string why;
-        if (!lower_system(system_, low, why)) {
+        if (system_.kind == SystemKind::LegacySpinGlass) {
+            low = legacy_model();
+        } else if (!lower_system(system_, low, why)) {
             result.diagnostics.add(StatusCode::UnsupportedExecution, why);
             return result;
         }

@@ -52,7 +52,7 @@ void release(hx_ctx* c)
                     c->hflip, c->vdiag, c->xi, c->counter, c->bath_off, c->error_flag, c->obs,
                     c->trace_buf, c->energy_buf, c->diag_table, c->ent_count, c->ent_slab, c->ent_bath,
                     c->ent_wc, c->ent_wa, c->order_perm, c->ado_keep, c->up_slot, c->up_ado, c->up_cnt,
-                    c->up_slab, c->up_bath, c->U};
+                    c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -106,10 +106,36 @@ hx::FusedArgs fused_args_of(const hx_ctx* c)
     return a;
 }
 
-// One stage: for d = 32, 64 the up-term kernel of tier L-1 followed by the
-// fused multi-CTA kernel; the generic kernel otherwise.  Returns kernels launched.
+hx::FlipArgs flip_args_of(const hx_ctx* c)
+{
+    hx::FlipArgs a{};
+    a.edges = c->edges;
+    a.acoef = c->acoef;
+    a.bcoef = c->bcoef;
+    a.gsum = c->gsum;
+    a.hdiag = c->hdiag;
+    a.hflip = c->hflip;
+    a.vdiag = c->vdiag;
+    a.vflip = c->vflip;
+    a.xi = c->xi;
+    a.counter = c->counter;
+    a.bath_off = c->bath_off;
+    a.H = c->H;
+    a.M = c->M;
+    a.J = c->J;
+    a.logd = c->logd;
+    return a;
+}
+
+// One stage: the two-pass flip path when V has spin-flip parts or d > 64; for
+// d = 32, 64 the up-term kernel of tier L-1 followed by the fused multi-CTA
+// kernel; the generic kernel otherwise.  Returns kernels launched.
 int launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
 {
+    if (c->use_flip) {
+        hx::launch_flip_stage(flip_args_of(c), u, c->Bbuf, rho, out, alpha, base, c->stream);
+        return 2;
+    }
     if (c->use_fused) {
         int k = 0;
         if (c->up_slots > 0) {
@@ -221,8 +247,8 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
         return fail(HX_ERR_INVALID_DIMENSION, "dim must be a power of two >= 2");
     int logd = 0;
     while ((1u << logd) < d) ++logd;
-    if (logd > hx::kMaxLogD)
-        return fail(HX_ERR_UNSUPPORTED_EXECUTION, "fused FP64 path supports dim <= 64");
+    if (logd > hx::kMaxLogDFlip)
+        return fail(HX_ERR_UNSUPPORTED_EXECUTION, "dim must be at most 4096");
     if (!p->h_diag) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "h_diag is NULL");
     if (p->precision != HX_PRECISION_DOUBLE)
         return fail(HX_ERR_UNSUPPORTED_PRECISION, "this entry point propagates in double precision only");
@@ -277,6 +303,20 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     c->stream = c->own_stream;
 
     const size_t nstate = static_cast<size_t>(H) * c->slab;
+    // spin-flip parts in any coupling operator select the two-pass flip path
+    std::vector<double> vf(static_cast<size_t>(J) * logd, 0.0);
+    bool any_flip = false;
+    for (int j = 0; j < J; ++j)
+        if (p->baths[j].coupling_flip)
+            for (int i = 0; i < logd; ++i) {
+                const double w = p->baths[j].coupling_flip[i];
+                if (!std::isfinite(w)) return fail(HX_ERR_UNSUPPORTED_BATH, "coupling flip weight is not finite");
+                vf[static_cast<size_t>(j) * logd + i] = w;
+                any_flip = any_flip || w != 0.0;
+            }
+    c->use_flip = any_flip || logd > hx::kMaxLogD;
+    if ((rc = dev_alloc(c, &c->vflip, vf.size())) || (rc = upload(c, c->vflip, vf))) return bail(rc);
+    if (c->use_flip && (rc = dev_alloc(c, &c->Bbuf, nstate * J))) return bail(rc);
     if ((rc = dev_alloc(c, &c->rho, nstate)) || (rc = dev_alloc(c, &c->ua, nstate)) ||
         (rc = dev_alloc(c, &c->ub, nstate)) || (rc = dev_alloc(c, &c->rows, H * M)) ||
         (rc = dev_alloc(c, &c->edges, H * 2 * M)) || (rc = dev_alloc(c, &c->acoef, H * M)) ||
@@ -345,7 +385,8 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     }
     // fused stage kernel (d = 32, 64): neighbour entry lists, diagonal table, up-term tables
     const char* force_generic = std::getenv("HX_FORCE_GENERIC_STAGE");
-    if (rc == HX_OK && logd >= 5 && hx::fused_supported(logd, M, J) && !(force_generic && force_generic[0] == '1')) {
+    if (rc == HX_OK && !c->use_flip && logd >= 5 && hx::fused_supported(logd, M, J) &&
+        !(force_generic && force_generic[0] == '1')) {
         cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
         int* dS = nullptr;
         if ((rc = dev_alloc(c, &c->diag_table, c->slab)) || (rc = dev_alloc(c, &c->ent_count, H)) ||
@@ -436,7 +477,7 @@ int hx_ctx_info(const hx_ctx* c, hx_info* info)
     info->device_bytes = c->device_bytes;
     info->steps_done = c->steps_done;
     info->time = static_cast<double>(c->steps_done) * c->dt;
-    info->kernels_per_step = static_cast<uint32_t>(c->order);
+    info->kernels_per_step = static_cast<uint32_t>(c->order) * ((c->use_flip || (c->use_fused && c->up_slots > 0)) ? 2 : 1);
     return HX_OK;
 }
 
@@ -464,7 +505,9 @@ int hx_ctx_sync(hx_ctx* c)
 int hx_ctx_step_trace(hx_ctx* c, uint64_t nsteps, double* rho0_trace, double* energy_trace)
 {
     if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
-    const int cap = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(nsteps, 1), 256));
+    // chunk of steps buffered on the device: at most 256 steps and 64 MB of rho_0 copies
+    const uint64_t by_bytes = std::max<uint64_t>(1, (uint64_t(64) << 20) / (c->slab * sizeof(double2)));
+    const int cap = static_cast<int>(std::min<uint64_t>(std::min<uint64_t>(std::max<uint64_t>(nsteps, 1), 256), by_bytes));
     if (c->trace_cap < cap) {
         if (c->trace_buf) cudaFree(c->trace_buf);
         if (c->energy_buf) cudaFree(c->energy_buf);
@@ -486,10 +529,11 @@ int hx_ctx_step_trace(hx_ctx* c, uint64_t nsteps, double* rho0_trace, double* en
         const int chunk = static_cast<int>(std::min<uint64_t>(nsteps - done, c->trace_cap));
         for (int t = 0; t < chunk; ++t) {
             enqueue_step(c);
-            hx::launch_observables(c->rho, c->logd, c->hdiag, c->hflip,
-                                   rho0_trace ? c->trace_buf + static_cast<size_t>(t) * c->slab : nullptr,
-                                   c->energy_buf + 3 * t, c->stream);
+            hx::launch_observables(c->rho, c->logd, c->hdiag, c->hflip, nullptr, c->energy_buf + 3 * t, c->stream);
             c->counters.kernel_launches += 1;
+            if (rho0_trace)
+                HX_CUDA_TRY(cudaMemcpyAsync(c->trace_buf + static_cast<size_t>(t) * c->slab, c->rho,
+                                            c->slab * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
         }
         int rc = check_launch("trace step");
         if (rc != HX_OK) return rc;

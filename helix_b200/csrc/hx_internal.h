@@ -51,7 +51,8 @@ uint64_t binom_u64(int n, int k);
 // Device-side parameter blocks
 // ---------------------------------------------------------------------------
 
-constexpr int kMaxLogD = 6;       // fused FP64 stage kernel: d <= 64
+constexpr int kMaxLogD = 6;       // slab-in-shared-memory stage kernels: d <= 64
+constexpr int kMaxLogDFlip = 12;  // flip-path stage kernels (hx_flip.cu): d <= 4096
 constexpr int kMaxModes = 128;
 constexpr int kMaxBaths = 64;
 
@@ -121,6 +122,26 @@ void launch_upterm_tables(const int32_t* rows, const int32_t* edges, const int32
                           int top, int32_t* slot, int* S_out, int32_t* ado, int* cnt, int32_t* slab, int32_t* bath,
                           cudaStream_t s);
 
+// Two-pass stage for coupling operators with spin-flip parts, any d (hx_flip.cu)
+struct FlipArgs {
+    const int32_t* edges;    // [H][2M]
+    const double* acoef;     // [H][M]
+    const double* bcoef;     // [H][J]
+    const double* gsum;      // [H]
+    const double* hdiag;     // [d]
+    const double* hflip;     // [log2 d]
+    const double* vdiag;     // [J][d]
+    const double* vflip;     // [J][log2 d]
+    const double* xi;        // [J]
+    const double* counter;   // [J]
+    const int32_t* bath_off; // [J+1]
+    long long H;
+    int M, J, logd;
+};
+// B (J * H * d*d complex) receives [V_j, u_n]; then out = base + alpha L(u).
+void launch_flip_stage(const FlipArgs& a, const double2* u, double2* B, const double2* rho, double2* out,
+                       double alpha, int base_kind, cudaStream_t s);
+
 // Tables on the device (hx_tables.cu)
 int build_tables_device(int M, int D, long long H, int32_t* d_rows, int32_t* d_edges, cudaStream_t s);
 // Same table kernel with a binomial table (rows n <= M + D, columns k <= M,
@@ -163,6 +184,9 @@ struct hx_ctx {
     double* hdiag = nullptr;
     double* hflip = nullptr;
     double* vdiag = nullptr;
+    double* vflip = nullptr;      // [J][log2 d]
+    bool use_flip = false;        // two-pass flip path (flips in V, or d > 64)
+    double2* Bbuf = nullptr;      // [J][H][d*d] commutators [V_j, u_n] (flip path)
     double* xi = nullptr;
     double* counter = nullptr;
     int32_t* bath_off = nullptr;

@@ -93,6 +93,11 @@ extern "C" int hx_rhs_noalloc(const hx_problem* p, const double* rho_device, dou
     if (p->max_depth < 1) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "max_depth must be >= 1");
 
     const int J = static_cast<int>(p->n_baths);
+    for (int j = 0; j < J; ++j)
+        if (p->baths[j].coupling_flip)
+            for (int i = 0; i < logd; ++i)
+                if (p->baths[j].coupling_flip[i] != 0.0)
+                    return fail(HX_ERR_UNSUPPORTED_BATH, "hx_rhs_noalloc supports diagonal coupling operators only");
     std::vector<hx::BathConst> bc(J);
     int M = 0;
     for (int j = 0; j < J; ++j) {

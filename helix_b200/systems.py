@@ -90,6 +90,7 @@ class BathSpec:
     K: int
     v_diag: np.ndarray | None = None
     v_csr: tuple | None = None  # (ptr, col, val complex) for non-diagonal V
+    v_flip: np.ndarray | None = None  # per-spin sigma_x weights of V (with v_diag)
 
     @staticmethod
     def drude_lorentz(lam: float, gamma: float, temperature: float, K: int, v_diag=None, v_csr=None):
@@ -153,12 +154,32 @@ class Problem:
 
     def bath_csr(self, j: int):
         b = self.baths[j]
+        if b.v_csr is None and b.v_flip is not None and np.any(np.asarray(b.v_flip) != 0):
+            return flip_operator_csr(self.dim, b.v_diag, b.v_flip)
         if b.v_csr is not None:
             ptr, col, val = b.v_csr
             return np.asarray(ptr, np.int32), np.asarray(col, np.int32), np.asarray(val, np.complex128)
         d = self.dim
         return (np.arange(d + 1, dtype=np.int32), np.arange(d, dtype=np.int32),
                 np.asarray(b.v_diag, np.float64).astype(np.complex128))
+
+
+def flip_operator_csr(dim: int, diag, flips):
+    """CSR of diag(diag) + sum_i flips[i] sigma_x(i), columns ascending."""
+    n = int(round(math.log2(dim)))
+    ptr = [0]
+    col: list[int] = []
+    val: list[complex] = []
+    for r in range(dim):
+        entries = {r: complex(diag[r])}
+        for i in range(n):
+            if flips[i] != 0.0:
+                entries[r ^ (1 << i)] = entries.get(r ^ (1 << i), 0.0) + complex(flips[i])
+        for c in sorted(entries):
+            col.append(c)
+            val.append(entries[c])
+        ptr.append(len(col))
+    return np.array(ptr, np.int32), np.array(col, np.int32), np.array(val, np.complex128)
 
 
 def hierarchy_size(modes: int, max_depth: int) -> int:
@@ -252,10 +273,25 @@ def legacy_v_csr(dim: int):
     return np.array(ptr, np.int32), np.array(col, np.int32), np.array(val, np.complex128)
 
 
+def legacy_v_parts(dim: int):
+    """Legacy V as (diagonal Dlong*sum(p), per-spin sigma_x weight Dtrans on the sparse flip masks)."""
+    n = int(round(math.log2(dim)))
+    diag = np.zeros(dim)
+    for row in range(dim):
+        psum = 0.0
+        for s in range(n):
+            psum += 0.5 * LEGACY["omega0"] if (row >> s) & 1 else -0.5 * LEGACY["omega0"]
+        diag[row] = LEGACY["dlong"] * psum
+    flips = np.array([LEGACY["dtrans"] if legacy_sparse_flip(1 << i) else 0.0 for i in range(n)])
+    return diag, flips
+
+
 def legacy_spin_glass(dim: int = 1024, dt: float | None = None) -> Problem:
     """The reference's compiled model at Hilbert size ``dim`` (default 1024)."""
     L = LEGACY
-    bath = BathSpec(beta=L["beta"], gamma=L["gamma"], zeta=L["zeta"], K=L["K"], v_csr=legacy_v_csr(dim))
+    vd, vf = legacy_v_parts(dim)
+    bath = BathSpec(beta=L["beta"], gamma=L["gamma"], zeta=L["zeta"], K=L["K"], v_csr=legacy_v_csr(dim),
+                    v_diag=vd, v_flip=vf)
     n = int(round(math.log2(dim)))
     return Problem(dim=dim, h_diag=legacy_h_diagonal(dim), h_flip=np.zeros(n), baths=[bath],
                    max_depth=L["jmax"], dt=L["dt"] if dt is None else dt, name=f"legacy_d{dim}")

@@ -47,22 +47,25 @@ extern "C" {
 #define HX_PRECISION_SINGLE 0
 #define HX_PRECISION_DOUBLE 1
 
-/* One Drude-Lorentz bath with Pade terms, coupled through a diagonal system
- * operator V_j.  Replaces the compiled bath of the reference
- * (src/parameters.cu:25-31; Bath, include/helix/types.h:108-128). */
+/* One Drude-Lorentz bath with Pade terms, coupled through the system operator
+ * V_j = diag(coupling_diag) + sum_i coupling_flip[i] * sigma_x(spin i).
+ * Replaces the compiled bath and coupling operator of the reference
+ * (src/parameters.cu:25-31; buildSparseOperators, src/initialize.cu:95-147;
+ * Bath, include/helix/types.h:108-128). */
 typedef struct hx_bath {
     double inverse_temperature; /* beta (Param::Betah) */
     double damping;             /* gamma (Param::Gamma) */
     double coupling_strength;   /* zeta (Param::Zeta); lambda = zeta*gamma/2 */
     uint32_t pade_terms;        /* K (Param::KMax) */
     const double* coupling_diag; /* dim real values: diagonal of V_j */
+    const double* coupling_flip; /* log2(dim) real values (sigma_x weights of V_j), or NULL */
 } hx_bath;
 
 /* One HEOM problem.  H = diag(h_diag) + sum_i h_flip[i] * sigma_x(spin i),
  * spin i <-> bit i of the basis index.  Replaces initialize()
  * (src/initialize.cu:342-353) and the compiled parameters it reads. */
 typedef struct hx_problem {
-    uint32_t dim;               /* Hilbert dimension d = 2^spins, 2 <= d <= 64 */
+    uint32_t dim;               /* Hilbert dimension d = 2^spins, 2 <= d <= 4096 */
     const double* h_diag;       /* d diagonal entries of H */
     const double* h_flip;       /* log2(d) transverse-field coefficients, or NULL */
     uint32_t n_baths;

@@ -31,7 +31,12 @@ int main(int argc, char** argv)
     solver.timeStep = dt;
     if (mode == "trace") solver.resultMode = helix::ResultMode::ObservableTrace;
     if (mode == "trajectory") solver.resultMode = helix::ResultMode::Trajectory;
-    if (mode == "legacy") system = helix::examples::legacy_spin_glass_system();
+    if (mode == "legacy") {
+        // the reference's example: compiled legacy system, bath and hierarchy
+        system = helix::examples::legacy_spin_glass_system();
+        hierarchy = helix::HierarchySpec::compiled_default(helix::Bath::drude_lorentz_pade());
+        options = helix::ContextOptions{};
+    }
     if (mode == "sparse-bad") {
         // a column index outside the operator: System::from_sparse validation must flag it
         helix::SparseOperator bad = system.couplings[0];

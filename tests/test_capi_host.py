@@ -55,7 +55,7 @@ def test_validation_errors_before_any_device_call():
     bad_dim = S.spin_glass(2, seed=1, depth=2, K=1)
     bad_dim.dim = 3
     assert _status_of(bad_dim) == "InvalidDimension"
-    big = S.spin_glass(7, seed=1, depth=1, K=0)
+    big = S.spin_glass(13, seed=1, depth=1, K=0)  # d = 8192 > 4096
     assert _status_of(big) == "UnsupportedExecution"
     nodepth = S.spin_glass(2, seed=1, depth=2, K=1)
     nodepth.max_depth = 0

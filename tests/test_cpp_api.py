@@ -31,9 +31,7 @@ def _run(exe, *args):
 
 
 def test_cpp_api_compiles_and_validates_without_device(exe):
-    # the legacy adapter and broken CSR input are rejected during validation
-    r = _run(exe, 3, 1, 1.0, 2, 1, 1, 0.01, "legacy")
-    assert r["ok"] is False and 9 in r["codes"]          # UnsupportedExecution
+    # broken CSR input is rejected during validation, before any device work
     r = _run(exe, 3, 1, 1.0, 2, 1, 1, 0.01, "sparse-bad")
     assert r["ok"] is False and 3 in r["codes"]          # InvalidColumnIndex
 
@@ -62,3 +60,23 @@ def test_cpp_api_matches_oracle(exe, mode):
         assert abs(r["energies"][0] - en_ref[-1]) <= 1e-10
     else:
         assert np.max(np.abs(np.array(r["energies"]) - en_ref)) <= 1e-10
+
+
+@pytest.mark.gpu
+def test_cpp_api_runs_the_reference_example(exe):
+    """The reference's own example (examples/cpp/legacy_spin_glass.cpp): the
+    compiled legacy system, compiled-default bath and hierarchy, 2 steps at the
+    default dt = 0.1; checked against the FP64 oracle."""
+    r = _run(exe, 0, 0, 0.0, 0, 0, 2, 0.1, "legacy")
+    assert r["ok"], r["codes"]
+    assert r["count"] == 1 and r["rows"] == 1024 and r["hierarchy"] == 10
+    assert r["times"] == [pytest.approx(0.2, abs=1e-15)]
+    rho = np.array(r["rho"]).view(np.complex128).reshape(1024, 1024)
+    p = S.legacy_spin_glass(1024)
+    o = O.Oracle(p)
+    o.run(2)
+    want = o.rho0()
+    e_ref = o.energy()
+    o.close()
+    assert np.max(np.abs(rho - want)) <= 1e-10
+    assert abs(r["energies"][0] - e_ref) <= 1e-10

@@ -1,0 +1,79 @@
+"""The reference's compiled model (collective V with spin flips) on the
+two-pass flip path: parity with the FP64 oracle, the reference's golden FP32
+energy trace (examples/outputEnergy.txt, tol 1e-5 as in CMakeLists.txt:1102-1115)
+and flip couplings on the spin-glass model."""
+import numpy as np
+import pytest
+
+from helix_b200 import capi
+from helix_b200 import systems as S
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+@pytest.mark.parametrize("dim", [4, 8, 32, 128])
+def test_legacy_model_rhs_and_steps_match_oracle(dim):
+    p = S.legacy_spin_glass(dim)
+    o = O.Oracle(p)
+    with capi.Context(p) as ctx:
+        assert ctx.size == 10
+        rng = np.random.default_rng(dim)
+        x = rng.standard_normal((10, dim, dim)) + 1j * rng.standard_normal((10, dim, dim))
+        ctx.set_state(x)
+        got = ctx.rhs()
+        want = o.rhs(x)
+        assert np.max(np.abs(got - want)) <= 1e-12 * max(1.0, np.max(np.abs(want)))
+        ctx.set_state(np.concatenate([S.initial_rho0(dim)[None], np.zeros((9, dim, dim))]))
+        rho, en = ctx.step_trace(15)
+    rho_ref, en_ref = o.run(15, trace=True)
+    assert np.max(np.abs(rho - rho_ref)) <= TOL
+    assert np.max(np.abs(en - en_ref)) <= TOL
+    o.close()
+
+
+def test_legacy_compiled_default_energy_trace(golden):
+    """d = 1024, 10 ADOs, dt = 0.1: the first 40 rows of the reference's golden
+    trace (FP32 reference, tolerance 1e-5) and 2 steps against the FP64 oracle."""
+    g = golden("legacy_energy_trace.json")
+    p = S.legacy_spin_glass(1024)
+    with capi.Context(p) as ctx:
+        e0, tr = ctx.observables()
+        assert abs(e0 - g["energy"][0]) < 1e-5 and abs(tr - 1.0) < 1e-14
+        rho, en = ctx.step_trace(40, rho0=True)
+    assert np.max(np.abs(en - np.array(g["energy"][1:41]))) < 1e-5
+    o = O.Oracle(p)
+    rho_ref, en_ref = o.run(2, trace=True)
+    o.close()
+    assert np.max(np.abs(rho[:2] - rho_ref)) <= TOL
+    assert np.max(np.abs(en[:2] - en_ref)) <= TOL
+
+
+def test_flip_coupling_on_spin_glass_matches_oracle():
+    """A transverse part in per-spin couplings (V_j = sz_j + 0.3 sx_j) selects the flip path for d = 16."""
+    p = S.spin_glass(4, seed=5, depth=2, K=1, h=0.8, dt=0.01)
+    for j, b in enumerate(p.baths):
+        f = np.zeros(4)
+        f[j] = 0.3
+        b.v_flip = f
+    o = O.Oracle(p)
+    rho_ref, en_ref = o.run(20, trace=True)
+    with capi.Context(p) as ctx:
+        rho, en = ctx.step_trace(20)
+    assert np.max(np.abs(rho - rho_ref)) <= TOL
+    assert np.max(np.abs(en - en_ref)) <= TOL
+    o.close()
+
+
+def test_large_dim_diagonal_coupling_uses_flip_path():
+    """d = 128 (> 64) with diagonal couplings runs on the flip path too."""
+    p = S.spin_glass(7, seed=3, depth=1, K=1, h=0.5, dt=0.01)
+    o = O.Oracle(p)
+    rho_ref, en_ref = o.run(5, trace=True)
+    with capi.Context(p) as ctx:
+        rho, en = ctx.step_trace(5)
+    assert np.max(np.abs(rho - rho_ref)) <= TOL
+    assert np.max(np.abs(en - en_ref)) <= TOL
+    o.close()
