@@ -222,9 +222,10 @@ def run_ours(args, cfg: dict) -> None:
     barrier()
     value = world * H * args.steps / (ms / 1000.0)
 
-    # roofline of the stage kernel: Horner form moves 11 state volumes per step
+    # roofline of one stage (one RHS evaluation with its Horner epilogue, all
+    # kernels of the stage): the Horner form moves 11 state volumes per step
     # (stage 1: read rho, write u1; stages 2-4: read u, read rho, write)
-    stages = int(ctx.info.kernels_per_step)
+    stages = 4
     alg_bytes_per_step = (3 * stages - 1) * state_bytes
     per_launch_bytes = alg_bytes_per_step / stages
     launch_ms = ms / (args.steps * stages)
