@@ -39,6 +39,8 @@ CONFIGS = {
                workload="spin_glass_d16_L3_K2_455ados_fp64"),
     # the reference's compiled default: d=1024, one collective bath (3 modes), 10 ADOs, dt=0.1
     "legacy": dict(legacy=True, dim=1024, workload="legacy_spin_glass_d1024_10ados_fp64"),
+    # batched disorder average: 512 seeded instances, N in {3,4,5}, L in {2,3,4}, K=2, dt=0.01
+    "c4": dict(batch=True, count=512, seed=2026, dt=0.01, workload="disorder_batch_512_N3-5_L2-4_K2_fp64"),
 }
 
 
@@ -146,6 +148,35 @@ def run_reference(args, cfg: dict) -> None:
     if rank != 0:
         return
     from oracle import oracle as O
+    if cfg.get("batch"):
+        # bounded sample of the batch: its first 16 instances of at most 1000 ADOs
+        sample = [q for q in S.disorder_batch(cfg["count"], cfg["seed"], dt=cfg["dt"])
+                  if q.hierarchy_size() <= 1000][:16]
+        ors = [O.Oracle(q) for q in sample]
+        for _ in range(args.warmup):
+            for o in ors:
+                o.run(1)
+        t0 = time.perf_counter()
+        for o in ors:
+            o.run(args.steps)
+        sec = time.perf_counter() - t0
+        size = sum(o.size for o in ors)
+        for o in ors:
+            o.close()
+        value = size * args.steps / sec
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "ados": size, "instances": len(sample), "dt": cfg["dt"],
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.threads(), "kind": "port",
+                             "sample": f"{len(sample)} instances (<= 1000 ADOs each), {args.steps} steps; the "
+                                       "reference has no CPU path, so its FP64 restatement stands in"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     p = make_problem(cfg)
     o = O.Oracle(p)
     for _ in range(args.warmup):
@@ -289,6 +320,166 @@ def run_ours(args, cfg: dict) -> None:
         dist.destroy_process_group()
 
 
+def run_batch(args, cfg: dict) -> None:
+    """Batched disorder average: instances sharded over ranks by state size
+    (no data-path collective), one persistent graph-captured launch per stage
+    on each rank, one all-reduce of the <sigma_z> sums at the end."""
+    import torch
+    import torch.distributed as dist
+
+    from helix_b200 import capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    problems = S.disorder_batch(cfg["count"], cfg["seed"], dt=cfg["dt"])
+    parts = S.shard_instances([S.state_bytes(p) for p in problems], world)
+    mine = [problems[i] for i in parts[rank]]
+    ados = sum(p.hierarchy_size() for p in mine)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    stream = torch.cuda.Stream()
+    b = capi.Batch(mine, tune=True)
+    b.set_stream(stream.cuda_stream)
+    st = b.info()
+    state_bytes = int(st.state_bytes)
+    b.step(args.warmup, trace=False)
+    b.sync()
+    l0 = int(b.info().kernel_launches)
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    b.step(args.steps, trace=False)
+    ev1.record(stream)
+    b.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    launches = int(b.info().kernel_launches) - l0
+    total_ados = sum(p.hierarchy_size() for p in problems)
+    value = total_ados * args.steps / (ms / 1000.0)
+    stage_ms = ms / (args.steps * 4)
+    per_stage_bytes = 11 * state_bytes / 4
+    achieved = per_stage_bytes / (stage_ms / 1000.0) / 1e9
+    peak, peak_kind = load_peaks()
+    b.close()
+
+    # end to end through the public API: create from host problems, step with
+    # the per-step disorder-average trace copied to the host, all-reduce
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b = capi.Batch(mine)
+    sz = b.step(args.steps)
+    b.close()
+    tot = torch.tensor(np.concatenate([sz, [len(mine)]]), device="cuda")
+    if world > 1:
+        dist.all_reduce(tot)
+    mean_sz = (tot[:-1] / tot[-1]).cpu().numpy()
+    e2e_sec = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = total_ados * args.steps / e2e_sec
+    h2d = sum(p.dim * (1 + len(p.baths)) * 8 + p.n_spins * 8 for p in mine)
+    assert np.all(np.isfinite(mean_sz)) and np.all(np.abs(mean_sz) <= 1.0 + 1e-9)
+
+    # plain FP64 form on the same GPU: every instance of this rank as its own
+    # context on its own stream (all in flight together), against the batch,
+    # both timed by the wall clock over the same steps
+    plain = None
+    if rank == 0 and not args.no_cpu_baseline:
+        n_plain = 10
+        ctxs = [capi.Context(p) for p in mine]
+        for c in ctxs:
+            c.step(2)
+        for c in ctxs:
+            c.sync()
+        t0 = time.perf_counter()
+        for c in ctxs:
+            c.step(n_plain)
+        for c in ctxs:
+            c.sync()
+        sec = time.perf_counter() - t0
+        plain_value = sum(c.size for c in ctxs) * n_plain / sec
+        for c in ctxs:
+            c.close()
+        bs = capi.Batch(mine, tune=True)
+        bs.step(2, trace=False)
+        bs.sync()
+        t0 = time.perf_counter()
+        bs.step(n_plain, trace=False)
+        bs.sync()
+        sec_b = time.perf_counter() - t0
+        batched_wall = ados * n_plain / sec_b
+        bs.close()
+        plain = {"plain_fp64_contexts": plain_value, "batched": batched_wall, "ratio": batched_wall / plain_value,
+                 "sample": f"all {len(mine)} instances of this rank, {n_plain} steps, wall clock after sync; "
+                           "plain = one hx_ctx and stream per instance"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        sample = [p for p in problems if p.hierarchy_size() <= 1000][:16]
+        ors = [O.Oracle(p) for p in sample]
+        for o in ors:
+            o.run(1)
+        t0 = time.perf_counter()
+        for o in ors:
+            o.run(args.cpu_steps * 10)
+        sec = time.perf_counter() - t0
+        cpu = {"value": sum(o.size for o in ors) * args.cpu_steps * 10 / sec, "unit": UNIT, "cores": O.threads(),
+               "kind": "port", "sample": f"{len(sample)} instances of the batch (<= 1000 ADOs each), "
+                                         f"{args.cpu_steps * 10} steps each, FP64 oracle, OpenMP"}
+        for o in ors:
+            o.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "instances": len(problems), "ados": total_ados,
+                       "ados_this_rank": ados, "dt": cfg["dt"], "integrator": "RK4 (4-term Taylor, Horner form)",
+                       "parallelism": f"instances sharded over {world} rank(s)" if world > 1 else "single",
+                       "tile_elems": int(st.tile_elems), "threads": int(st.threads), "grid": int(st.grid),
+                       "l2": f"inputs larger than L2 (state {state_bytes / 1e9:.3f} GB per rank)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None,
+                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                         else "fallback 6650 GB/s",
+                         "algorithmic_bytes_per_launch": per_stage_bytes, "kernel": "batch_stage_kernel",
+                         "launch_ms": stage_ms},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+                    "d2h_bytes_per_step": 8,
+                    "path": "hx_batch_create (host problems) + hx_batch_step (<sigma_z> sum per step to host) + all-reduce"},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "disorder_average_sz_final": float(mean_sz[-1]),
+        }
+        if plain is not None:
+            line["plain_fp64_same_gpu"] = plain
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -302,6 +493,8 @@ def main() -> None:
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         run_reference(args, cfg)
+    elif cfg.get("batch"):
+        run_batch(args, cfg)
     else:
         run_ours(args, cfg)
 

@@ -32,6 +32,8 @@ EXPORTS = [
     "hx_ctx_info", "hx_ctx_counters", "hx_ctx_step", "hx_ctx_step_trace", "hx_ctx_sync",
     "hx_ctx_read_rho0", "hx_ctx_observables", "hx_ctx_read_state", "hx_ctx_write_state",
     "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_check_finite", "hx_rhs_noalloc",
+    "hx_batch_create", "hx_batch_destroy", "hx_batch_set_stream", "hx_batch_info", "hx_batch_tune",
+    "hx_batch_step", "hx_batch_sync", "hx_batch_read_rho0",
 ]
 
 
@@ -64,6 +66,18 @@ class Info(C.Structure):
 class Counters(C.Structure):
     _fields_ = [("kernel_launches", C.c_uint64), ("stage_launches", C.c_uint64),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("observable_spin", C.c_uint32), ("tune", C.c_uint32), ("tile_elems", C.c_uint32),
+                ("threads", C.c_uint32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("tile_elems", C.c_uint32), ("total_ados", C.c_uint64),
+                ("state_bytes", C.c_uint64), ("device_bytes", C.c_uint64), ("steps_done", C.c_uint64),
+                ("kernel_launches", C.c_uint64), ("threads", C.c_uint32), ("tiles", C.c_uint32),
+                ("grid", C.c_uint32), ("kernels_per_step", C.c_uint32)]
 
 
 _lib = None
@@ -110,6 +124,15 @@ def lib():
             L.hx_ctx_rhs.argtypes = [vp, vp, u64]
             L.hx_ctx_check_finite.argtypes = [vp]
             L.hx_rhs_noalloc.argtypes = [C.POINTER(_Problem), vp, vp, vp]
+            L.hx_batch_create.argtypes = [C.POINTER(_Problem), u32, C.POINTER(BatchOptions), C.POINTER(vp)]
+            L.hx_batch_destroy.argtypes = [vp]
+            L.hx_batch_destroy.restype = None
+            L.hx_batch_set_stream.argtypes = [vp, vp]
+            L.hx_batch_info.argtypes = [vp, C.POINTER(BatchStats)]
+            L.hx_batch_tune.argtypes = [vp, C.POINTER(u32), C.POINTER(u32)]
+            L.hx_batch_step.argtypes = [vp, u64, vp]
+            L.hx_batch_sync.argtypes = [vp]
+            L.hx_batch_read_rho0.argtypes = [vp, u32, vp, u64]
             _lib = L
         return _lib
 
@@ -300,3 +323,76 @@ class Context:
 
     def check_finite(self) -> None:
         _check(lib().hx_ctx_check_finite(self._h))
+
+
+class Batch:
+    """Many independent instances propagated together (wraps hx_batch).
+
+    ``step(n, trace=True)`` returns, per step, the sum over instances of
+    <sigma_z(spin)> of rho_0; divide by ``count`` (or by the total count over
+    all ranks after an all-reduce) for the disorder average.
+    """
+
+    def __init__(self, problems, order: int = 4, spin: int = 0, tune: bool = False, tile_elems: int = 0,
+                 threads: int = 0):
+        L = lib()
+        self.problems = list(problems)
+        structs = (_Problem * len(self.problems))()
+        self._keep = []
+        for i, p in enumerate(self.problems):
+            st, keep = _problem_struct(p, order)
+            structs[i] = st
+            self._keep += keep
+        self._keep.append(structs)
+        opt = BatchOptions(spin, 1 if tune else 0, tile_elems, threads)
+        h = C.c_void_p()
+        _check(L.hx_batch_create(structs, len(self.problems), C.byref(opt), C.byref(h)))
+        self._h = h
+        self.count = len(self.problems)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().hx_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> BatchStats:
+        st = BatchStats()
+        _check(lib().hx_batch_info(self._h, C.byref(st)))
+        return st
+
+    def tune(self) -> tuple[int, int]:
+        a, b = C.c_uint32(), C.c_uint32()
+        _check(lib().hx_batch_tune(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        _check(lib().hx_batch_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def step(self, nsteps: int, trace: bool = True):
+        out = np.zeros(nsteps) if trace else None
+        _check(lib().hx_batch_step(self._h, nsteps, _p(out) if trace else None))
+        return out
+
+    def step_into(self, nsteps: int, out: np.ndarray | None) -> None:
+        _check(lib().hx_batch_step(self._h, nsteps, None if out is None else _p(out)))
+
+    def sync(self) -> None:
+        _check(lib().hx_batch_sync(self._h))
+
+    def rho0(self, i: int) -> np.ndarray:
+        d = self.problems[i].dim
+        out = np.zeros((d, d), np.complex128)
+        _check(lib().hx_batch_read_rho0(self._h, i, _p(out), 2 * out.size))
+        return out

@@ -82,7 +82,9 @@ hx::StageTables tables_of(const hx_ctx* c)
     return t;
 }
 
-hx::FusedArgs fused_args_of(const hx_ctx* c)
+}  // namespace
+
+hx::FusedArgs hx::fused_args_of(const hx_ctx* c)
 {
     hx::FusedArgs a{};
     a.diag = c->diag_table;
@@ -105,6 +107,13 @@ hx::FusedArgs fused_args_of(const hx_ctx* c)
     a.logd = c->logd;
     return a;
 }
+
+hx::UpTermArgs hx::upterm_args_of(const hx_ctx* c)
+{
+    return hx::UpTermArgs{c->vdiag, c->up_cnt, c->up_slab, c->up_bath, c->bath_off, c->up_slots, c->M, c->J, c->logd};
+}
+
+namespace {
 
 hx::FlipArgs flip_args_of(const hx_ctx* c)
 {
@@ -139,11 +148,10 @@ int launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* o
     if (c->use_fused) {
         int k = 0;
         if (c->up_slots > 0) {
-            hx::UpTermArgs ua{c->vdiag, c->up_cnt, c->up_slab, c->up_bath, c->bath_off, c->up_slots, c->M, c->J, c->logd};
-            hx::launch_upterm(ua, u, c->U, c->stream);
+            hx::launch_upterm(hx::upterm_args_of(c), u, c->U, c->stream);
             ++k;
         }
-        if (hx::launch_fused(fused_args_of(c), u, rho, out, alpha, base, c->stream)) return k + 1;
+        if (hx::launch_fused(hx::fused_args_of(c), u, rho, out, alpha, base, c->stream)) return k + 1;
     }
     hx::launch_stage(tables_of(c), u, rho, out, alpha, base, c->stream);
     return 1;

@@ -101,10 +101,10 @@ __device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity)
     return false;
 }
 
-template <int LOGD, int MINB>
-__global__ void __launch_bounds__(256, MINB)
-    fused_kernel(FusedArgs a, const double2* __restrict__ u, const double2* rho, double2* out, double alpha,
-                 int base_kind)
+// The stage of ADO n: out_n = base_n + alpha L(u)_n (one CTA of 256 threads).
+template <int LOGD>
+__device__ __forceinline__ void fused_ado(const FusedArgs& a, long long n, const double2* __restrict__ u,
+                                          const double2* rho, double2* out, double alpha, int base_kind)
 {
     constexpr int D = 1 << LOGD, D2 = D * D, T = 256;
     constexpr int E = D2 / T;         // elements per thread
@@ -122,7 +122,6 @@ __global__ void __launch_bounds__(256, MINB)
     int* sBath = sSlab + 2 * a.M;
 
     const int tid = threadIdx.x;
-    const long long n = a.order ? static_cast<long long>(a.order[blockIdx.x]) : static_cast<long long>(blockIdx.x);
     const uint64_t pk = pol_last(), pn = pol_normal();
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(&bar[0])) : "memory");
@@ -272,6 +271,15 @@ __global__ void __launch_bounds__(256, MINB)
     }
 }
 
+template <int LOGD, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    fused_kernel(FusedArgs a, const double2* __restrict__ u, const double2* rho, double2* out, double alpha,
+                 int base_kind)
+{
+    const long long n = a.order ? static_cast<long long>(a.order[blockIdx.x]) : static_cast<long long>(blockIdx.x);
+    fused_ado<LOGD>(a, n, u, rho, out, alpha, base_kind);
+}
+
 template <int LOGD>
 size_t fused_smem(int M, int J)
 {
@@ -279,11 +287,12 @@ size_t fused_smem(int M, int J)
     return D * D * sizeof(double2) + 16 + sizeof(double) * (J * D + LOGD + 4 * M) + sizeof(int) * 4 * M;
 }
 
+// Raise the kernel's dynamic shared-memory limit to what (M, J) needs, once
+// per device (a function attribute; must not happen during stream capture).
 template <int LOGD, int MINB>
-bool launch3(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha, int base,
-             cudaStream_t s)
+bool prepare3(int M, int J)
 {
-    const size_t smem = fused_smem<LOGD>(a.M, a.J);
+    const size_t smem = fused_smem<LOGD>(M, J);
     if (smem > 227 * 1024) return false;
     static size_t configured[64] = {};
     int dev = 0;
@@ -294,6 +303,15 @@ bool launch3(const FusedArgs& a, const double2* u, const double2* rho, double2* 
             return false;
         configured[dev] = smem;
     }
+    return true;
+}
+
+template <int LOGD, int MINB>
+bool launch3(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha, int base,
+             cudaStream_t s)
+{
+    const size_t smem = fused_smem<LOGD>(a.M, a.J);
+    if (!prepare3<LOGD, MINB>(a.M, a.J)) return false;
     fused_kernel<LOGD, MINB><<<static_cast<unsigned>(a.H), 256, smem, s>>>(a, u, rho, out, alpha, base);
     return true;
 }
@@ -365,6 +383,15 @@ bool launch_fused(const FusedArgs& a, const double2* u, const double2* rho, doub
     switch (a.logd) {
     case 5: return launch3<5, 3>(a, u, rho, out, alpha, base_kind, s);
     case 6: return launch3<6, 2>(a, u, rho, out, alpha, base_kind, s);
+    default: return false;
+    }
+}
+
+bool prepare_fused(int logd, int M, int J)
+{
+    switch (logd) {
+    case 5: return prepare3<5, 3>(M, J);
+    case 6: return prepare3<6, 2>(M, J);
     default: return false;
     }
 }

@@ -9,6 +9,8 @@
 
 #include "helix_b200.h"
 
+struct hx_ctx;
+
 namespace hx {
 
 // Thread-local last-error text behind hx_last_error().
@@ -100,6 +102,7 @@ struct FusedArgs {
     int M, J, logd;
 };
 bool fused_supported(int logd, int M, int J);
+bool prepare_fused(int logd, int M, int J);  // raises the shared-memory limit; call before stream capture
 bool launch_fused(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
                   int base_kind, cudaStream_t s);
 void launch_entries(const int32_t* rows, const int32_t* edges, const double* acoef, const double* bcoef,
@@ -118,9 +121,14 @@ struct UpTermArgs {
     int S, M, J, logd;
 };
 void launch_upterm(const UpTermArgs& a, const double2* u, double2* U, cudaStream_t s);
+
 void launch_upterm_tables(const int32_t* rows, const int32_t* edges, const int32_t* mode_bath, long long H, int M,
                           int top, int32_t* slot, int* S_out, int32_t* ado, int* cnt, int32_t* slab, int32_t* bath,
                           cudaStream_t s);
+
+// Argument blocks of a context's fused and up-term kernels (hx_ctx.cu)
+FusedArgs fused_args_of(const ::hx_ctx* c);
+UpTermArgs upterm_args_of(const ::hx_ctx* c);
 
 // Two-pass stage for coupling operators with spin-flip parts, any d (hx_flip.cu)
 struct FlipArgs {

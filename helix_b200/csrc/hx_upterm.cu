@@ -29,18 +29,18 @@ constexpr int kTile = 32;          // elements per tile (one per lane)
 // ADO has its up neighbour in the top tier and the up weight -i delta_j is
 // the same for all modes of bath j, so each bath's neighbour slabs are summed
 // unweighted and -i delta_j is applied once.
-__global__ void __launch_bounds__(kWarps * 32)
-    upterm_kernel(UpTermArgs a, const double2* __restrict__ u, double2* __restrict__ U)
+__device__ __forceinline__ void upterm_block(const UpTermArgs& a, int bx, int by, const double2* __restrict__ u,
+                                             double2* __restrict__ U)
 {
     const int D = 1 << a.logd;
     const long long D2 = static_cast<long long>(D) * D;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const long long e = static_cast<long long>(blockIdx.y) * kTile + lane;
+    const long long e = static_cast<long long>(by) * kTile + lane;
     const int r = static_cast<int>(e >> a.logd);
     const int c = static_cast<int>(e & (D - 1));
     const double2* ue = u + e;
-    const int s0 = (blockIdx.x * kWarps + warp) * kSlotsPerWarp;
+    const int s0 = (bx * kWarps + warp) * kSlotsPerWarp;
     for (int s = s0; s < s0 + kSlotsPerWarp && s < a.S; ++s) {
         const int32_t* slab = a.slab + static_cast<long long>(s) * a.M;
         double re = 0.0, im = 0.0;
@@ -59,6 +59,12 @@ __global__ void __launch_bounds__(kWarps * 32)
         }
         U[static_cast<long long>(s) * D2 + e] = make_double2(re, im);
     }
+}
+
+__global__ void __launch_bounds__(kWarps * 32)
+    upterm_kernel(UpTermArgs a, const double2* __restrict__ u, double2* __restrict__ U)
+{
+    upterm_block(a, blockIdx.x, blockIdx.y, u, U);
 }
 
 // slot[i] = rank of ADO i among tier L-1 ADOs (or -1); per slot, its up

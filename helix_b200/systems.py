@@ -211,6 +211,52 @@ def spin_glass(n_spins: int, seed: int, h: float = 1.0, lam: float = 0.1, gamma:
                    meta={"seed": seed, "J": J, "h": h, "lam": lam, "T": temperature, "depth": depth})
 
 
+def disorder_instance(seed: int, dt: float = 0.01, K: int = 2, gamma: float = 1.0) -> Problem:
+    """One realisation of the batched disorder average.
+
+    From splitmix64(seed), in this order: N ~ U{3,4,5} spins, depth
+    L ~ U{2,3,4}, h ~ U(0.5,1.5), lambda ~ U(0.05,0.2), T ~ U(0.5,2.0); then
+    J_ij ~ N(0,1) for i<j in row-major pair order from the same stream.  Every
+    spin has its own Drude-Lorentz bath (lambda, gamma=1, T, Pade K).
+    """
+    rng = SplitMix64(seed)
+    n = rng.randint(3, 5)
+    depth = rng.randint(2, 4)
+    h = rng.uniform_range(0.5, 1.5)
+    lam = rng.uniform_range(0.05, 0.2)
+    temp = rng.uniform_range(0.5, 2.0)
+    J = np.zeros((n, n))
+    for i in range(n):
+        for j in range(i + 1, n):
+            J[i, j] = J[j, i] = rng.normal()
+    p = spin_glass(n, seed, h=h, lam=lam, gamma=gamma, temperature=temp, K=K, depth=depth, dt=dt, J=J)
+    p.name = f"disorder_{seed}"
+    return p
+
+
+def disorder_batch(count: int, seed: int, dt: float = 0.01, K: int = 2) -> list[Problem]:
+    """Instances seed, seed+1, ..., seed+count-1 (disorder_instance)."""
+    return [disorder_instance(seed + i, dt=dt, K=K) for i in range(count)]
+
+
+def state_bytes(p: Problem) -> int:
+    return p.hierarchy_size() * p.dim * p.dim * 16
+
+
+def shard_instances(sizes, world: int) -> list[list[int]]:
+    """Greedy longest-first partition of instance indices over ``world`` ranks
+    by state size; ties go to the lowest rank, so every rank computes the same
+    partition.  Each rank's list is in ascending instance order."""
+    order = sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i))
+    load = [0] * world
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += int(sizes[i])
+    return [sorted(p) for p in parts]
+
+
 # Legacy compiled-model constants (src/parameters.cu:11-31)
 LEGACY = dict(omega0=1.0, dlong=1.0, dtrans=1.0, jnaver=0.6, beta=3.0, gamma=1.0, zeta=0.01,
               K=2, jmax=3, dt=0.1)

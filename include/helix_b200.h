@@ -197,6 +197,60 @@ int hx_ctx_rhs(hx_ctx* ctx, double* out, uint64_t n);
  * HX_ERR_NON_FINITE otherwise. */
 int hx_ctx_check_finite(hx_ctx* ctx);
 
+/* ------------------------------------------------------------------------
+ * Batches: many independent instances in one persistent launch per stage.
+ * The reference runs one instance per HEOMSolver::run (src/helix.cpp:723-772)
+ * and has no batched mode; a batch is that call for hundreds of disorder
+ * realisations of uneven size at once, with the disorder average of
+ * <sigma_z(spin)> reduced on the device every step.
+ * ------------------------------------------------------------------------ */
+typedef struct hx_batch hx_batch;
+
+typedef struct hx_batch_options {
+    uint32_t observable_spin; /* spin whose <sigma_z> is averaged (bit index), default 0 */
+    uint32_t tune;            /* 1 = run the tile-shape autotuner at creation */
+    uint32_t tile_elems;      /* elements per tile (power of two, 64..8192); 0 = 2048 */
+    uint32_t threads;         /* threads per CTA (multiple of 32, 64..1024); 0 = 256 */
+} hx_batch_options;
+
+typedef struct hx_batch_stats {
+    uint32_t count;           /* instances */
+    uint32_t tile_elems;
+    uint64_t total_ados;
+    uint64_t state_bytes;     /* bytes of one state of all instances */
+    uint64_t device_bytes;
+    uint64_t steps_done;
+    uint64_t kernel_launches; /* kernels launched by stepping and tuning so far */
+    uint32_t threads;
+    uint32_t tiles;
+    uint32_t grid;            /* persistent CTAs per stage launch */
+    uint32_t kernels_per_step;
+} hx_batch_stats;
+
+/* Create a batch from `count` problems on the current device.  Every problem
+ * has 2 <= dim <= 64, diagonal coupling operators, at most 64 modes, and all
+ * share time_step and integration_order; each starts in |d-1><d-1|. */
+int hx_batch_create(const hx_problem* problems, uint32_t count, const hx_batch_options* options,
+                    hx_batch** out);
+void hx_batch_destroy(hx_batch* batch);
+int hx_batch_set_stream(hx_batch* batch, void* stream);
+int hx_batch_info(const hx_batch* batch, hx_batch_stats* info);
+
+/* Time every candidate tile shape on this batch (three stage launches each,
+ * the state untouched) and keep the fastest; reports the choice. */
+int hx_batch_tune(hx_batch* batch, uint32_t* tile_elems, uint32_t* threads);
+
+/* Advance every instance `nsteps` steps (a captured CUDA graph per step).
+ * If sz_sum_trace is not NULL, sz_sum_trace[t] receives, after step t, the
+ * sum over instances of Tr(sigma_z(spin) rho_0) (divide by the instance count
+ * for the disorder average; sums add across batches on several GPUs) and the
+ * call returns when they have landed; otherwise it returns at once. */
+int hx_batch_step(hx_batch* batch, uint64_t nsteps, double* sz_sum_trace);
+int hx_batch_sync(hx_batch* batch);
+
+/* rho_0 of one instance (d*d complex, row-major) into a host buffer of n doubles. */
+int hx_batch_read_rho0(hx_batch* batch, uint32_t instance, double* out, uint64_t n);
+
 /* One evaluation of the right-hand side, drho = L(rho) for every ADO, that
  * allocates no memory.  No counterpart in the reference.
  *
