@@ -39,6 +39,9 @@ CONFIGS = {
                workload="spin_glass_d16_L3_K2_455ados_fp64"),
     # the reference's compiled default: d=1024, one collective bath (3 modes), 10 ADOs, dt=0.1
     "legacy": dict(legacy=True, dim=1024, workload="legacy_spin_glass_d1024_10ados_fp64"),
+    # mixed precision: N=8 (d=256), h=0.5, Pade K=1 (16 modes), depth L=3 -> 969 ADOs, dt=0.005, 500 steps
+    "c3": dict(n=8, depth=3, K=1, h=0.5, dt=0.005, seed=2027, mixed=True, error_steps=500,
+               workload="spin_glass_d256_L3_K1_969ados_complex64_mixed"),
     # batched disorder average: 512 seeded instances, N in {3,4,5}, L in {2,3,4}, K=2, dt=0.01
     "c4": dict(batch=True, count=512, seed=2026, dt=0.01, workload="disorder_batch_512_N3-5_L2-4_K2_fp64"),
 }
@@ -480,6 +483,129 @@ def run_batch(args, cfg: dict) -> None:
         dist.destroy_process_group()
 
 
+def run_mixed(args, cfg: dict) -> None:
+    """Mixed precision (complex64 hierarchy, rho_0 in FP64) against the plain
+    FP64 propagator on the same GPU; error = trace distance of rho_0 against
+    the FP64 run over the configuration's full step count."""
+    import torch
+
+    from helix_b200 import capi
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1 and rank != 0:
+        return  # one hierarchy: the comparison runs on one GPU
+    p = make_problem(cfg, 0)
+    stream = torch.cuda.Stream()
+
+    def timed(precision: str):
+        ctx = capi.Context(p, precision=precision)
+        ctx.set_stream(stream.cuda_stream)
+        for _ in range(args.warmup):
+            ctx.step(1)
+        ctx.sync()
+        c0 = ctx.counters()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        ctx.step(args.steps)
+        ev1.record(stream)
+        ctx.sync()
+        torch.cuda.synchronize()
+        launches = int(ctx.counters().kernel_launches - c0.kernel_launches)
+        info = ctx.get_info()
+        ctx.close()
+        return ev0.elapsed_time(ev1), launches, info
+
+    ms64, _, info64 = timed("double")
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, launches, info = timed("mixed")
+    clk = clocks.stop()
+    H = int(info.hierarchy_size)
+    value = H * args.steps / (ms / 1000.0)
+    plain = H * args.steps / (ms64 / 1000.0)
+    state32 = H * p.dim * p.dim * 8
+    per_stage = 11 * state32 / 4
+    stage_ms = ms / (args.steps * 4)
+    achieved = per_stage / (stage_ms / 1000.0) / 1e9
+    peak, peak_kind = load_peaks()
+
+    # error against the FP64 propagator, every 10 steps over the full run
+    def trace_distance(a, b):
+        m = a - b
+        return 0.5 * float(np.sum(np.abs(np.linalg.eigvalsh(0.5 * (m + m.conj().T)))))
+
+    n_err = cfg["error_steps"]
+    c64 = capi.Context(p)
+    cm = capi.Context(p, precision="mixed")
+    td, en_err = [], []
+    for _ in range(n_err // 10):
+        r64, e64 = c64.step_trace(10)
+        rm, em = cm.step_trace(10)
+        td.append(trace_distance(rm[-1], r64[-1]))
+        en_err.append(float(np.max(np.abs(em - e64))))
+    c64.close()
+    cm.close()
+
+    # end to end through the C ABI: state upload from host, steps with rho_0(t)
+    # and <H>(t) to the host, final rho_0
+    pinned = torch.empty(H * p.dim * p.dim * 2, dtype=torch.float64, pin_memory=True)
+    host_state = pinned.numpy().view(np.complex128).reshape(H, p.dim, p.dim)
+    host_state[:] = 0
+    host_state[0] = S.initial_rho0(p.dim)
+    rho_trace = torch.empty(args.steps * p.dim * p.dim * 2, dtype=torch.float64, pin_memory=True).numpy()
+    en_trace = np.zeros(args.steps)
+    ctx = capi.Context(p, precision="mixed")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.set_state(host_state)
+    ctx.step_trace_into(args.steps, rho_trace, en_trace)
+    ctx.rho0()
+    e2e_sec = time.perf_counter() - t0
+    ctx.close()
+    e2e_value = H * args.steps / e2e_sec
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        o = O.Oracle(p)
+        t0 = time.perf_counter()
+        o.run(1)
+        sec = time.perf_counter() - t0
+        o.close()
+        cpu = {"value": H / sec, "unit": UNIT, "cores": O.threads(), "kind": "port",
+               "sample": f"1 full step of the {H}-ADO hierarchy, FP64 oracle, OpenMP"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 (rho_0 f64)", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "ados": H, "dim": p.dim, "modes": p.modes, "depth_L": p.max_depth - 1,
+                   "dt": p.dt, "integrator": "RK4 (4-term Taylor, Horner form)", "parallelism": "single",
+                   "l2": f"inputs larger than L2 (state {state32 / 1e9:.3f} GB complex64)"},
+        "plain_fp64_same_gpu": {"value": plain, "ms_per_step": ms64 / args.steps, "speedup": value / plain},
+        "error_vs_fp64": {"trace_distance_max": max(td), "trace_distance_final": td[-1],
+                          "energy_abs_max": max(en_err), "steps": n_err, "every": 10},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None,
+                     "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                     else "fallback 6650 GB/s",
+                     "algorithmic_bytes_per_launch": per_stage, "kernel": "large_kernel<float,8> + large_upterm_kernel",
+                     "launch_ms": stage_ms},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": H * p.dim * p.dim * 16 / args.steps,
+                "d2h_bytes_per_step": p.dim * p.dim * 16 + 24,
+                "path": "hx_ctx_write_state + hx_ctx_step_trace (rho0, <H> per step) + hx_ctx_read_rho0"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -495,6 +621,8 @@ def main() -> None:
         run_reference(args, cfg)
     elif cfg.get("batch"):
         run_batch(args, cfg)
+    elif cfg.get("mixed"):
+        run_mixed(args, cfg)
     else:
         run_ours(args, cfg)
 

@@ -24,6 +24,7 @@ STATUS_NAMES = {
     18: "DeviceWaitTimeout",
 }
 PRECISION_DOUBLE = 1
+PRECISION_MIXED = 2  # complex64 hierarchy, ADO 0 (rho_0) in double precision
 
 # Every exported symbol of include/helix_b200.h
 EXPORTS = [
@@ -178,7 +179,7 @@ def seeded_couplings(n: int, seed: int) -> np.ndarray:
     return J
 
 
-def _problem_struct(problem, order: int = 4, dt: float | None = None):
+def _problem_struct(problem, order: int = 4, dt: float | None = None, precision: int = PRECISION_DOUBLE):
     """hx_problem for a systems.Problem; returns (struct, keep-alive list)."""
     d = problem.dim
     n = problem.n_spins
@@ -205,7 +206,7 @@ def _problem_struct(problem, order: int = 4, dt: float | None = None):
     keep.append(baths)
     prob = _Problem(d, hd.ctypes.data_as(C.POINTER(C.c_double)), hf.ctypes.data_as(C.POINTER(C.c_double)),
                     len(problem.baths), baths, problem.max_depth, problem.dt if dt is None else dt, order,
-                    PRECISION_DOUBLE, 0)
+                    precision, 0)
     return prob, keep
 
 
@@ -220,11 +221,12 @@ def rhs_noalloc(problem, rho_device_ptr: int, drho_device_ptr: int, stream_ptr: 
 class Context:
     """One HEOM problem resident on the current CUDA device (wraps hx_ctx)."""
 
-    def __init__(self, problem, order: int = 4, dt: float | None = None):
+    def __init__(self, problem, order: int = 4, dt: float | None = None, precision: str = "double"):
         L = lib()
         self.problem = problem
         d = problem.dim
-        prob, self._keep = _problem_struct(problem, order, dt)
+        prec = {"double": PRECISION_DOUBLE, "mixed": PRECISION_MIXED}[precision]
+        prob, self._keep = _problem_struct(problem, order, dt, prec)
         h = C.c_void_p()
         _check(L.hx_ctx_create(C.byref(prob), C.byref(h)))
         self._h = h

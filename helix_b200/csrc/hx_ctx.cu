@@ -52,7 +52,8 @@ void release(hx_ctx* c)
                     c->hflip, c->vdiag, c->xi, c->counter, c->bath_off, c->error_flag, c->obs,
                     c->trace_buf, c->energy_buf, c->diag_table, c->ent_count, c->ent_slab, c->ent_bath,
                     c->ent_wc, c->ent_wa, c->order_perm, c->ado_keep, c->up_slot, c->up_ado, c->up_cnt,
-                    c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf};
+                    c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf, c->rho32, c->ua32, c->ub32,
+                    c->U32, c->diag32, c->vdiag32, c->hflip32};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -136,11 +137,102 @@ hx::FlipArgs flip_args_of(const hx_ctx* c)
     return a;
 }
 
+hx::LargeArgs<double> large_args64(const hx_ctx* c)
+{
+    hx::LargeArgs<double> a{};
+    a.diag = c->diag_table;
+    a.vdiag = c->vdiag;
+    a.hflip = c->hflip;
+    a.gsum = c->gsum;
+    a.ent_count = c->ent_count;
+    a.ent_slab = c->ent_slab;
+    a.ent_bath = c->ent_bath;
+    a.ent_wc = c->ent_wc;
+    a.ent_wa = c->ent_wa;
+    a.slot = c->up_slot;
+    a.U = c->U;
+    a.error_flag = c->error_flag;
+    a.H = c->H;
+    a.M = c->M;
+    a.J = c->J;
+    a.logd = c->logd;
+    a.first_ado = 0;
+    return a;
+}
+
+hx::LargeArgs<float> large_args32(const hx_ctx* c)
+{
+    hx::LargeArgs<float> a{};
+    a.diag = c->diag32;
+    a.vdiag = c->vdiag32;
+    a.hflip = c->hflip32;
+    a.gsum = c->gsum;
+    a.ent_count = c->ent_count;
+    a.ent_slab = c->ent_slab;
+    a.ent_bath = c->ent_bath;
+    a.ent_wc = c->ent_wc;
+    a.ent_wa = c->ent_wa;
+    a.slot = c->up_slot;
+    a.U = c->U32;
+    a.error_flag = c->error_flag;
+    a.H = c->H;
+    a.M = c->M;
+    a.J = c->J;
+    a.logd = c->logd;
+    a.first_ado = 1;
+    return a;
+}
+
+template <typename R>
+hx::LargeUpArgs<R> large_up_args(const hx_ctx* c, const R* vdiag)
+{
+    return hx::LargeUpArgs<R>{vdiag, c->up_slab, c->bath_off, c->up_slots, c->M, c->J, c->logd};
+}
+
+hx::Ado0Args ado0_args(const hx_ctx* c)
+{
+    return hx::Ado0Args{c->diag_table, c->vdiag, c->hflip, c->ent_count, c->ent_slab, c->ent_bath,
+                        c->ent_wc, c->ent_wa, c->M, c->J, c->logd};
+}
+
+// Index of a state buffer of the context: 0 = rho, 1 = ua, 2 = ub.
+int buffer_id(const hx_ctx* c, const double2* p) { return p == c->rho ? 0 : (p == c->ua ? 1 : 2); }
+
+// One stage of the band kernels (hx_large.cu): the up-term kernel of tier
+// L-1, the band kernel over the hierarchy and, in mixed precision, the
+// double-precision kernel of ADO 0.  Returns kernels launched.
+int launch_large_stage(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
+{
+    int k = 0;
+    if (!c->mixed) {
+        if (c->up_slots > 0) {
+            hx::launch_large_upterm<double>(large_up_args<double>(c, c->vdiag), u, c->U, c->stream);
+            ++k;
+        }
+        hx::launch_large<double>(large_args64(c), u, rho, out, alpha, base, c->stream);
+        return k + 1;
+    }
+    float2* b32[3] = {c->rho32, c->ua32, c->ub32};
+    const float2* u32 = b32[buffer_id(c, u)];
+    float2* o32 = b32[buffer_id(c, out)];
+    if (c->up_slots > 0) {
+        hx::launch_large_upterm<float>(large_up_args<float>(c, c->vdiag32), u32, c->U32, c->stream);
+        ++k;
+    }
+    if (c->H > 1) {
+        hx::launch_large<float>(large_args32(c), u32, c->rho32, o32, alpha, base, c->stream);
+        ++k;
+    }
+    hx::launch_ado0(ado0_args(c), u, u32, rho, out, o32, alpha, base, c->stream);
+    return k + 1;
+}
+
 // One stage: the two-pass flip path when V has spin-flip parts or d > 64; for
 // d = 32, 64 the up-term kernel of tier L-1 followed by the fused multi-CTA
 // kernel; the generic kernel otherwise.  Returns kernels launched.
 int launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
 {
+    if (c->use_large) return launch_large_stage(c, u, rho, out, alpha, base);
     if (c->use_flip) {
         hx::launch_flip_stage(flip_args_of(c), u, c->Bbuf, rho, out, alpha, base, c->stream);
         return 2;
@@ -165,6 +257,7 @@ int enqueue_step(hx_ctx* c)
     if (m == 1) {
         launched += launch_stage_any(c, c->rho, c->rho, c->ua, c->dt, hx::kBaseSelf);
         std::swap(c->rho, c->ua);
+        if (c->mixed) std::swap(c->rho32, c->ua32);
     } else {
         const double2* in = c->rho;
         double2* bufs[2] = {c->ua, c->ub};
@@ -197,6 +290,24 @@ int read_error_flag(hx_ctx* c)
         cudaMemsetAsync(c->error_flag, 0, sizeof(int), c->stream);
         return fail(HX_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration budget");
     }
+    return HX_OK;
+}
+
+// Mixed precision: the whole state as complex128 on the host (complex64
+// hierarchy widened, ADO 0 from its double-precision slab); src32/src64 are
+// matching buffers (rho32/rho, ua32/ua, ...).
+int read_mixed(hx_ctx* c, const float2* src32, const double2* src64, double* out)
+{
+    const size_t count = static_cast<size_t>(c->H) * c->slab;
+    std::vector<float2> tmp(count);
+    HX_CUDA_TRY(cudaMemcpyAsync(tmp.data(), src32, count * sizeof(float2), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA_TRY(cudaMemcpyAsync(out, src64, c->slab * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (size_t i = c->slab; i < count; ++i) {
+        out[2 * i] = tmp[i].x;
+        out[2 * i + 1] = tmp[i].y;
+    }
+    c->counters.d2h_bytes += count * sizeof(float2) + c->slab * sizeof(double2);
     return HX_OK;
 }
 
@@ -258,8 +369,10 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     if (logd > hx::kMaxLogDFlip)
         return fail(HX_ERR_UNSUPPORTED_EXECUTION, "dim must be at most 4096");
     if (!p->h_diag) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "h_diag is NULL");
-    if (p->precision != HX_PRECISION_DOUBLE)
-        return fail(HX_ERR_UNSUPPORTED_PRECISION, "this entry point propagates in double precision only");
+    if (p->precision != HX_PRECISION_DOUBLE && p->precision != HX_PRECISION_MIXED)
+        return fail(HX_ERR_UNSUPPORTED_PRECISION, "precision must be HX_PRECISION_DOUBLE or HX_PRECISION_MIXED");
+    if (p->precision == HX_PRECISION_MIXED && (logd < 7 || logd > 10 || p->max_depth < 3))
+        return fail(HX_ERR_UNSUPPORTED_PRECISION, "mixed precision needs 128 <= dim <= 1024 and max_depth >= 3");
     if (!(p->time_step > 0.0) || !std::isfinite(p->time_step))
         return fail(HX_ERR_INVALID_RUNTIME_OPTION, "time_step must be positive");
     if (p->integration_order < 1 || p->integration_order > 8)
@@ -322,11 +435,20 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                 vf[static_cast<size_t>(j) * logd + i] = w;
                 any_flip = any_flip || w != 0.0;
             }
-    c->use_flip = any_flip || logd > hx::kMaxLogD;
+    c->use_large = !any_flip && logd >= 7 && hx::large_supported(logd, M, J);
+    c->use_flip = any_flip || (logd > hx::kMaxLogD && !c->use_large);
+    c->mixed = p->precision == HX_PRECISION_MIXED;
+    if (c->mixed && !c->use_large)
+        return bail(fail(HX_ERR_UNSUPPORTED_PRECISION, "mixed precision needs diagonal coupling operators"));
     if ((rc = dev_alloc(c, &c->vflip, vf.size())) || (rc = upload(c, c->vflip, vf))) return bail(rc);
     if (c->use_flip && (rc = dev_alloc(c, &c->Bbuf, nstate * J))) return bail(rc);
-    if ((rc = dev_alloc(c, &c->rho, nstate)) || (rc = dev_alloc(c, &c->ua, nstate)) ||
-        (rc = dev_alloc(c, &c->ub, nstate)) || (rc = dev_alloc(c, &c->rows, H * M)) ||
+    // double-precision state: the whole hierarchy, or only ADO 0 in mixed precision
+    const size_t n64 = c->mixed ? c->slab : nstate;
+    if (c->mixed && ((rc = dev_alloc(c, &c->rho32, nstate)) || (rc = dev_alloc(c, &c->ua32, nstate)) ||
+                     (rc = dev_alloc(c, &c->ub32, nstate))))
+        return bail(rc);
+    if ((rc = dev_alloc(c, &c->rho, n64)) || (rc = dev_alloc(c, &c->ua, n64)) ||
+        (rc = dev_alloc(c, &c->ub, n64)) || (rc = dev_alloc(c, &c->rows, H * M)) ||
         (rc = dev_alloc(c, &c->edges, H * 2 * M)) || (rc = dev_alloc(c, &c->acoef, H * M)) ||
         (rc = dev_alloc(c, &c->bcoef, H * J)) || (rc = dev_alloc(c, &c->gsum, H)) ||
         (rc = dev_alloc(c, &c->hdiag, d)) || (rc = dev_alloc(c, &c->hflip, logd)) ||
@@ -388,13 +510,19 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     if (rc == HX_OK) {
         hx::launch_coefficients(c->rows, c->H, M, J, dmb, dmk, dnu, dtc, dta, dphi, c->bath_off, c->acoef,
                                 c->bcoef, c->gsum, c->stream);
-        hx::launch_init_state(c->rho, static_cast<long long>(nstate), c->d, c->stream);
+        hx::launch_init_state(c->rho, static_cast<long long>(n64), c->d, c->stream);
+        if (c->mixed) {
+            e = cudaMemsetAsync(c->rho32, 0, nstate * sizeof(float2), c->stream);
+            if (e == cudaSuccess) hx::launch_d2f(c->rho, c->rho32, static_cast<long long>(c->slab), c->stream);
+            if (e != cudaSuccess) rc = hx::cuda_fail(e, "mixed initial state");
+        }
         rc = check_launch("setup kernels");
     }
     // fused stage kernel (d = 32, 64): neighbour entry lists, diagonal table, up-term tables
     const char* force_generic = std::getenv("HX_FORCE_GENERIC_STAGE");
-    if (rc == HX_OK && !c->use_flip && logd >= 5 && hx::fused_supported(logd, M, J) &&
-        !(force_generic && force_generic[0] == '1')) {
+    const bool fused_ok = !c->use_flip && !c->use_large && logd >= 5 && logd <= hx::kMaxLogD &&
+                          hx::fused_supported(logd, M, J) && !(force_generic && force_generic[0] == '1');
+    if (rc == HX_OK && (fused_ok || c->use_large)) {
         cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
         int* dS = nullptr;
         if ((rc = dev_alloc(c, &c->diag_table, c->slab)) || (rc = dev_alloc(c, &c->ent_count, H)) ||
@@ -423,7 +551,10 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                 if (e == cudaSuccess && S > 0) {
                     rc = dev_alloc(c, &c->up_slab, static_cast<size_t>(S) * M);
                     if (rc == HX_OK) rc = dev_alloc(c, &c->up_bath, static_cast<size_t>(S) * M);
-                    if (rc == HX_OK) rc = dev_alloc(c, &c->U, static_cast<size_t>(S) * c->slab);
+                    if (rc == HX_OK) {
+                        if (c->mixed) rc = dev_alloc(c, &c->U32, static_cast<size_t>(S) * c->slab);
+                        else rc = dev_alloc(c, &c->U, static_cast<size_t>(S) * c->slab);
+                    }
                     if (rc == HX_OK) {
                         e = cudaMemcpyAsync(c->up_slab, tmp_slab, static_cast<size_t>(S) * M * sizeof(int32_t),
                                             cudaMemcpyDeviceToDevice, c->stream);
@@ -441,7 +572,18 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                 if (e != cudaSuccess) rc = hx::cuda_fail(e, "up-term tables");
             }
             c->up_slots = S;
-            c->use_fused = (rc == HX_OK);
+            c->use_fused = (rc == HX_OK) && fused_ok;
+            // single-precision copies of the operators for the mixed band kernel
+            if (rc == HX_OK && c->mixed) {
+                if ((rc = dev_alloc(c, &c->diag32, c->slab)) || (rc = dev_alloc(c, &c->vdiag32, static_cast<size_t>(J) * d)) ||
+                    (rc = dev_alloc(c, &c->hflip32, logd))) {
+                } else {
+                    hx::launch_d2f(c->diag_table, c->diag32, static_cast<long long>(c->slab), c->stream);
+                    hx::launch_vec_d2f(c->vdiag, c->vdiag32, static_cast<long long>(J) * d, c->stream);
+                    hx::launch_vec_d2f(c->hflip, c->hflip32, logd, c->stream);
+                    rc = check_launch("mixed-precision operators");
+                }
+            }
         }
         cudaFree(dS);
         if (dS) c->device_bytes -= sizeof(int);
@@ -452,6 +594,16 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     cudaFree(dphi);
     cudaFree(dtc);
     cudaFree(dta);
+    if (rc == HX_OK && c->use_large && (c->diag_table == nullptr || c->ent_count == nullptr))
+        rc = fail(HX_ERR_UNSUPPORTED_EXECUTION, "band-kernel tables were not built");
+    if (rc == HX_OK && c->use_large) {
+        const bool ok = c->mixed ? hx::prepare_large<float>(large_args32(c)) : hx::prepare_large<double>(large_args64(c));
+        if (!ok) rc = fail(HX_ERR_UNSUPPORTED_EXECUTION, "band kernel does not fit in shared memory");
+    }
+    if (rc == HX_OK) {
+        e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) rc = hx::cuda_fail(e, "context set-up");
+    }
     if (rc != HX_OK) return bail(rc);
     c->counters.kernel_launches += 3;
     *out = c;
@@ -485,7 +637,9 @@ int hx_ctx_info(const hx_ctx* c, hx_info* info)
     info->device_bytes = c->device_bytes;
     info->steps_done = c->steps_done;
     info->time = static_cast<double>(c->steps_done) * c->dt;
-    info->kernels_per_step = static_cast<uint32_t>(c->order) * ((c->use_flip || (c->use_fused && c->up_slots > 0)) ? 2 : 1);
+    int per_stage = (c->use_flip || (c->use_fused && c->up_slots > 0)) ? 2 : 1;
+    if (c->use_large) per_stage = 1 + (c->up_slots > 0 ? 1 : 0) + (c->mixed ? 1 : 0);
+    info->kernels_per_step = static_cast<uint32_t>(c->order) * per_stage;
     return HX_OK;
 }
 
@@ -596,6 +750,10 @@ int hx_ctx_read_state(hx_ctx* c, double* out, uint64_t n)
     if (!c || !out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
     const size_t count = static_cast<size_t>(c->H) * c->slab;
     if (n < 2 * count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "output buffer too small");
+    if (c->mixed) {
+        const int rc = read_mixed(c, c->rho32, c->rho, out);
+        return rc != HX_OK ? rc : read_error_flag(c);
+    }
     HX_CUDA_TRY(cudaMemcpyAsync(out, c->rho, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->counters.d2h_bytes += count * sizeof(double2);
@@ -607,6 +765,16 @@ int hx_ctx_write_state(hx_ctx* c, const double* in, uint64_t n)
     if (!c || !in) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
     const size_t count = static_cast<size_t>(c->H) * c->slab;
     if (n < 2 * count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "input buffer too small");
+    if (c->mixed) {
+        std::vector<float2> tmp(count);
+        for (size_t i = 0; i < count; ++i)
+            tmp[i] = make_float2(static_cast<float>(in[2 * i]), static_cast<float>(in[2 * i + 1]));
+        HX_CUDA_TRY(cudaMemcpyAsync(c->rho32, tmp.data(), count * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+        HX_CUDA_TRY(cudaMemcpyAsync(c->rho, in, c->slab * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        c->counters.h2d_bytes += count * sizeof(float2) + c->slab * sizeof(double2);
+        HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return HX_OK;
+    }
     HX_CUDA_TRY(cudaMemcpyAsync(c->rho, in, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
     c->counters.h2d_bytes += count * sizeof(double2);
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -628,6 +796,10 @@ int hx_ctx_rhs(hx_ctx* c, double* out, uint64_t n)
     c->counters.kernel_launches += launch_stage_any(c, c->rho, c->rho, c->ua, 1.0, hx::kBaseZero);
     int rc = check_launch("stage kernel launch");
     if (rc != HX_OK) return rc;
+    if (c->mixed) {
+        rc = read_mixed(c, c->ua32, c->ua, out);
+        return rc != HX_OK ? rc : read_error_flag(c);
+    }
     HX_CUDA_TRY(cudaMemcpyAsync(out, c->ua, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return read_error_flag(c);
@@ -636,6 +808,14 @@ int hx_ctx_rhs(hx_ctx* c, double* out, uint64_t n)
 int hx_ctx_check_finite(hx_ctx* c)
 {
     if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
+    if (c->mixed) {
+        std::vector<double> all(2 * static_cast<size_t>(c->H) * c->slab);
+        const int rc = read_mixed(c, c->rho32, c->rho, all.data());
+        if (rc != HX_OK) return rc;
+        for (double v : all)
+            if (!std::isfinite(v)) return fail(HX_ERR_NON_FINITE, "state holds non-finite values");
+        return read_error_flag(c);
+    }
     int host = 0;
     int* scratch = reinterpret_cast<int*>(c->obs + 3);
     HX_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(int), c->stream));

@@ -126,6 +126,60 @@ void launch_upterm_tables(const int32_t* rows, const int32_t* edges, const int32
                           int top, int32_t* slot, int* S_out, int32_t* ado, int* cnt, int32_t* slab, int32_t* bath,
                           cudaStream_t s);
 
+// Stage kernels for 128 <= d <= 1024 with diagonal couplings, in double or
+// in single precision with complex64 storage (hx_large.cu)
+template <typename R> struct C2Of;
+template <> struct C2Of<double> { using type = double2; };
+template <> struct C2Of<float> { using type = float2; };
+template <typename R> using C2 = typename C2Of<R>::type;
+
+template <typename R>
+struct LargeArgs {
+    const C2<R>* diag;       // [d*d] ADO-independent diagonal coefficient table
+    const R* vdiag;          // [J][d]
+    const R* hflip;          // [log2 d]
+    const double* gsum;      // [H]
+    const int* ent_count;    // [H]
+    const int32_t* ent_slab; // [H][2M]
+    const int32_t* ent_bath; // [H][2M] bath (low 16 bits)
+    const double* ent_wc;    // [H][2M]
+    const double* ent_wa;    // [H][2M]
+    const int32_t* slot;     // [H] slot of a tier L-1 ADO in U, else -1
+    const C2<R>* U;          // [S][d*d]
+    int* error_flag;
+    long long H;
+    int M, J, logd;
+    int first_ado;           // 1 when ADO 0 runs in double precision (ado0_kernel)
+};
+template <typename R>
+struct LargeUpArgs {
+    const R* vdiag;          // [J][d]
+    const int32_t* slab;     // [S][M]
+    const int32_t* bath_off; // [J+1]
+    int S, M, J, logd;
+};
+struct Ado0Args {
+    const double2* diag;     // [d*d]
+    const double* vdiag;     // [J][d]
+    const double* hflip;     // [log2 d]
+    const int* ent_count;    // entries of ADO 0 (first row of the context's tables)
+    const int32_t* ent_slab;
+    const int32_t* ent_bath;
+    const double* ent_wc;
+    const double* ent_wa;
+    int M, J, logd;
+};
+bool large_supported(int logd, int M, int J);
+template <typename R> bool prepare_large(const LargeArgs<R>& a);  // shared-memory limit; call before capture
+template <typename R>
+bool launch_large(const LargeArgs<R>& a, const C2<R>* u, const C2<R>* rho, C2<R>* out, double alpha, int base_kind,
+                  cudaStream_t s);
+template <typename R> void launch_large_upterm(const LargeUpArgs<R>& a, const C2<R>* u, C2<R>* U, cudaStream_t s);
+void launch_ado0(const Ado0Args& a, const double2* u0, const float2* u, const double2* rho0, double2* out0,
+                 float2* out32, double alpha, int base_kind, cudaStream_t s);
+void launch_d2f(const double2* in, float2* out, long long n, cudaStream_t s);
+void launch_vec_d2f(const double* in, float* out, long long n, cudaStream_t s);
+
 // Argument blocks of a context's fused and up-term kernels (hx_ctx.cu)
 FusedArgs fused_args_of(const ::hx_ctx* c);
 UpTermArgs upterm_args_of(const ::hx_ctx* c);
@@ -193,7 +247,16 @@ struct hx_ctx {
     double* hflip = nullptr;
     double* vdiag = nullptr;
     double* vflip = nullptr;      // [J][log2 d]
-    bool use_flip = false;        // two-pass flip path (flips in V, or d > 64)
+    bool use_flip = false;        // two-pass flip path (flips in V, or d > 1024)
+    bool use_large = false;       // band kernels for 128 <= d <= 1024, diagonal V (hx_large.cu)
+    bool mixed = false;           // complex64 hierarchy, ADO 0 in double precision
+    float2* rho32 = nullptr;      // mixed: complex64 state buffers (rho, ua, ub mirror them)
+    float2* ua32 = nullptr;
+    float2* ub32 = nullptr;
+    float2* U32 = nullptr;        // mixed: up terms of tier L-1
+    float2* diag32 = nullptr;
+    float* vdiag32 = nullptr;
+    float* hflip32 = nullptr;
     double2* Bbuf = nullptr;      // [J][H][d*d] commutators [V_j, u_n] (flip path)
     double* xi = nullptr;
     double* counter = nullptr;

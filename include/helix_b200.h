@@ -46,6 +46,12 @@ extern "C" {
 
 #define HX_PRECISION_SINGLE 0
 #define HX_PRECISION_DOUBLE 1
+/* Mixed precision: complex64 hierarchy state and single-precision
+ * right-hand side, the tier-0 ADO (the reduced density matrix), its energy and
+ * trace in double precision.  Needs 128 <= dim <= 1024, diagonal coupling
+ * operators and max_depth >= 3.  No counterpart in the reference, whose
+ * precision is fixed at compile time (src/legacy_compile_options.h:6). */
+#define HX_PRECISION_MIXED 2
 
 /* One Drude-Lorentz bath with Pade terms, coupled through the system operator
  * V_j = diag(coupling_diag) + sum_i coupling_flip[i] * sigma_x(spin i).
@@ -73,7 +79,7 @@ typedef struct hx_problem {
     uint32_t max_depth;         /* exclusive bound on sum(n) */
     double time_step;           /* dt (Param::Step) */
     uint32_t integration_order; /* Taylor order (Param::IntegrationNum), 1..8 */
-    uint32_t precision;         /* HX_PRECISION_DOUBLE */
+    uint32_t precision;         /* HX_PRECISION_DOUBLE or HX_PRECISION_MIXED */
     uint32_t flags;             /* reserved, 0 */
 } hx_problem;
 
@@ -185,7 +191,8 @@ int hx_ctx_read_state(hx_ctx* ctx, double* out, uint64_t n);
 int hx_ctx_write_state(hx_ctx* ctx, const double* in, uint64_t n);
 
 /* Device pointer of the state (hierarchy_size * d * d double2), for callers
- * that fill or read it on the device. */
+ * that fill or read it on the device.  In mixed precision this is the
+ * double-precision slab of ADO 0 only (d * d double2). */
 int hx_ctx_state_device_ptr(hx_ctx* ctx, void** ptr);
 
 /* One evaluation of the right-hand side L(rho) of the current state into a

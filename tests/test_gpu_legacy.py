@@ -67,8 +67,8 @@ def test_flip_coupling_on_spin_glass_matches_oracle():
     o.close()
 
 
-def test_large_dim_diagonal_coupling_uses_flip_path():
-    """d = 128 (> 64) with diagonal couplings runs on the flip path too."""
+def test_large_dim_diagonal_coupling_matches_oracle():
+    """d = 128 (> 64) with diagonal couplings (band kernels of hx_large.cu)."""
     p = S.spin_glass(7, seed=3, depth=1, K=1, h=0.5, dt=0.01)
     o = O.Oracle(p)
     rho_ref, en_ref = o.run(5, trace=True)
