@@ -42,6 +42,11 @@ CONFIGS = {
     # mixed precision: N=8 (d=256), h=0.5, Pade K=1 (16 modes), depth L=3 -> 969 ADOs, dt=0.005, 500 steps
     "c3": dict(n=8, depth=3, K=1, h=0.5, dt=0.005, seed=2027, mixed=True, error_steps=500,
                workload="spin_glass_d256_L3_K1_969ados_complex64_mixed"),
+    # learned closure: N=5 (d=32), K=2 (15 modes), L=2 + MLP closure of tier 3; trained on 64 seeds of plain
+    # L=5 FP64 runs (dt=0.01, 1000 steps), tested on 16 held-out seeds against plain L=5
+    "c5": dict(n=5, K=2, h=1.0, dt=0.01, closure=True, coarse_depth=2, fine_depth=5, train_seeds=64,
+               test_seeds=16, traj_steps=1000, every=50, hidden=512, iters=6000, mlp_batch=1024, lr=1e-3,
+               workload="spin_glass_d32_K2_L2_plus_mlp_closure_vs_L5"),
     # batched disorder average: 512 seeded instances, N in {3,4,5}, L in {2,3,4}, K=2, dt=0.01
     "c4": dict(batch=True, count=512, seed=2026, dt=0.01, workload="disorder_batch_512_N3-5_L2-4_K2_fp64"),
 }
@@ -606,6 +611,107 @@ def run_mixed(args, cfg: dict) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_closure(args, cfg: dict) -> None:
+    """Learned closure: L=2 hierarchy + MLP closure of tier 3 against the plain
+    L=5 run (the judge) and the plain truncated L=2 run, on held-out seeds.
+    value = closure ADO-steps/s of the coarse hierarchy; the line also gives
+    the simulated-steps rate of closure and of plain L=5 and the trace
+    distances of rho_0(t)."""
+    import torch
+
+    from helix_b200 import capi
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and rank != 0:
+        return
+    n, K, dt = cfg["n"], cfg["K"], cfg["dt"]
+    steps, every = cfg["traj_steps"], cfg["every"]
+
+    def problem(seed, depth):
+        return S.spin_glass(n, seed=seed, depth=depth, K=K, h=cfg["h"], dt=dt)
+
+    def td(a, b):
+        m = a - b
+        return 0.5 * float(np.sum(np.abs(np.linalg.eigvalsh(0.5 * (m + m.conj().T)))))
+
+    train_seeds = [5000 + i for i in range(cfg["train_seeds"])]
+    test_seeds = [9000 + i for i in range(cfg["test_seeds"])]
+    t0 = time.perf_counter()
+    cl = capi.Closure(problem(train_seeds[0], cfg["coarse_depth"]), fine_max_depth=cfg["fine_depth"] + 1,
+                      hidden=cfg["hidden"], capacity=len(train_seeds) * steps // every, seed=1)
+    for s in train_seeds:
+        with capi.Context(problem(s, cfg["fine_depth"])) as ctx:
+            for _ in range(steps // every):
+                ctx.step(every)
+                cl.harvest(ctx)
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss = cl.train(iters=cfg["iters"], batch=cfg["mlp_batch"], lr=cfg["lr"], seed=7)
+    t_train = time.perf_counter() - t0
+    info = cl.info()
+
+    # held-out seeds: plain L=5 (judge), plain L=2, L=2 + closure; device-timed runs
+    stream = torch.cuda.Stream()
+
+    def run(p, closure=None, timed=True):
+        ctx = capi.Context(p)
+        ctx.set_stream(stream.cuda_stream)
+        if closure is not None:
+            closure.attach(ctx)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        rho, _ = ctx.step_trace(steps, rho0=True, energy=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        H = ctx.size
+        ctx.close()
+        return rho, ev0.elapsed_time(ev1), H
+
+    e_plain, e_closed, ms_fine, ms_closed, ms_plain = [], [], 0.0, 0.0, 0.0
+    clocks = ClockSampler(local)
+    clocks.start()
+    for s in test_seeds:
+        ref, mf, H_fine = run(problem(s, cfg["fine_depth"]))
+        plain, mp, _ = run(problem(s, cfg["coarse_depth"]))
+        closed, mc, H_coarse = run(problem(s, cfg["coarse_depth"]), cl)
+        ms_fine += mf
+        ms_plain += mp
+        ms_closed += mc
+        e_plain.append(max(td(plain[t], ref[t]) for t in range(0, steps, 10)))
+        e_closed.append(max(td(closed[t], ref[t]) for t in range(0, steps, 10)))
+    clk = clocks.stop()
+    cl.close()
+    nt = len(test_seeds)
+    value = H_coarse * steps * nt / (ms_closed / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps * nt, "warmup": 0,
+        "ms_per_step": ms_closed / (steps * nt), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 hierarchy, bf16 MLP (f32 accumulation)", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "ados_coarse": H_coarse, "ados_fine": H_fine, "dim": 1 << n,
+                   "modes": 3 * n, "coarse_depth_L": cfg["coarse_depth"], "fine_depth_L": cfg["fine_depth"],
+                   "dt": dt, "train_seeds": len(train_seeds), "test_seeds": nt, "trajectory_steps": steps,
+                   "snapshot_every": every, "mlp": f"{info['top_ados']}x{3 * n} pairs per RHS, "
+                   f"{2 * (1 << n) ** 2 + 3 * n}-{cfg['hidden']}-{cfg['hidden']}-{2 * (1 << n) ** 2} GELU",
+                   "parallelism": "single"},
+        "closure": {"simulated_steps_per_s": steps * nt / (ms_closed / 1000.0),
+                    "plain_fine_steps_per_s": steps * nt / (ms_fine / 1000.0),
+                    "plain_coarse_steps_per_s": steps * nt / (ms_plain / 1000.0),
+                    "speedup_vs_plain_fine": ms_fine / ms_closed,
+                    "trace_distance_vs_fine": {"closure_max": max(e_closed), "closure_mean": float(np.mean(e_closed)),
+                                               "truncated_max": max(e_plain), "truncated_mean": float(np.mean(e_plain))},
+                    "gain_over_truncation": float(np.mean(e_plain) / np.mean(e_closed)),
+                    "train": {"snapshots": info["snapshots"], "data_s": t_data, "train_s": t_train,
+                              "iters": cfg["iters"], "batch": cfg["mlp_batch"], "loss_first": float(loss[:20].mean()),
+                              "loss_last": float(loss[-100:].mean())}},
+        "gpu_launches": None,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -623,6 +729,8 @@ def main() -> None:
         run_batch(args, cfg)
     elif cfg.get("mixed"):
         run_mixed(args, cfg)
+    elif cfg.get("closure"):
+        run_closure(args, cfg)
     else:
         run_ours(args, cfg)
 

@@ -35,6 +35,10 @@ EXPORTS = [
     "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_check_finite", "hx_rhs_noalloc",
     "hx_batch_create", "hx_batch_destroy", "hx_batch_set_stream", "hx_batch_info", "hx_batch_tune",
     "hx_batch_step", "hx_batch_sync", "hx_batch_read_rho0",
+    "hx_mlp_create", "hx_mlp_destroy", "hx_mlp_num_params", "hx_mlp_get_params", "hx_mlp_set_params",
+    "hx_mlp_forward", "hx_mlp_gradients", "hx_mlp_train", "hx_closure_create", "hx_closure_destroy",
+    "hx_closure_mlp", "hx_closure_info", "hx_closure_harvest", "hx_closure_train", "hx_closure_set_scales",
+    "hx_ctx_set_closure",
 ]
 
 
@@ -134,6 +138,24 @@ def lib():
             L.hx_batch_step.argtypes = [vp, u64, vp]
             L.hx_batch_sync.argtypes = [vp]
             L.hx_batch_read_rho0.argtypes = [vp, u32, vp, u64]
+            L.hx_mlp_create.argtypes = [u32, u32, u32, u64, C.POINTER(vp)]
+            L.hx_mlp_destroy.argtypes = [vp]
+            L.hx_mlp_destroy.restype = None
+            L.hx_mlp_num_params.argtypes = [vp, C.POINTER(u64)]
+            L.hx_mlp_get_params.argtypes = [vp, vp, u64]
+            L.hx_mlp_set_params.argtypes = [vp, vp, u64]
+            L.hx_mlp_forward.argtypes = [vp, vp, u32, vp]
+            L.hx_mlp_gradients.argtypes = [vp, vp, vp, u32, C.POINTER(C.c_float), vp, u64]
+            L.hx_mlp_train.argtypes = [vp, vp, vp, u32, u32, u32, C.c_float, u64, vp]
+            L.hx_closure_create.argtypes = [C.POINTER(_Problem), u32, u32, u32, u64, C.POINTER(vp)]
+            L.hx_closure_destroy.argtypes = [vp]
+            L.hx_closure_destroy.restype = None
+            L.hx_closure_mlp.argtypes = [vp, C.POINTER(vp)]
+            L.hx_closure_info.argtypes = [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), dp, dp]
+            L.hx_closure_harvest.argtypes = [vp, vp]
+            L.hx_closure_train.argtypes = [vp, u32, u32, C.c_float, u64, vp]
+            L.hx_closure_set_scales.argtypes = [vp, C.c_double, C.c_double]
+            L.hx_ctx_set_closure.argtypes = [vp, vp]
             _lib = L
         return _lib
 
@@ -398,3 +420,112 @@ class Batch:
         out = np.zeros((d, d), np.complex128)
         _check(lib().hx_batch_read_rho0(self._h, i, _p(out), 2 * out.size))
         return out
+
+
+class MLP:
+    """The closure network (wraps hx_mlp); host buffers in float32."""
+
+    def __init__(self, in_dim: int, hidden: int, out_dim: int, seed: int = 0, handle=None, owner=None):
+        self.in_dim, self.hidden, self.out_dim = in_dim, hidden, out_dim
+        self._owner = owner
+        if handle is None:
+            h = C.c_void_p()
+            _check(lib().hx_mlp_create(in_dim, hidden, out_dim, seed, C.byref(h)))
+            self._h, self._owned = h, True
+        else:
+            self._h, self._owned = handle, False
+        n = C.c_uint64()
+        _check(lib().hx_mlp_num_params(self._h, C.byref(n)))
+        self.n_params = int(n.value)
+
+    def close(self):
+        if self._owned and getattr(self, "_h", None) and self._h.value:
+            lib().hx_mlp_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.n_params, np.float32)
+        _check(lib().hx_mlp_get_params(self._h, _p(out), self.n_params))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        _check(lib().hx_mlp_set_params(self._h, _p(p), p.size))
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros((x.shape[0], self.out_dim), np.float32)
+        _check(lib().hx_mlp_forward(self._h, _p(x), x.shape[0], _p(y)))
+        return y
+
+    def gradients(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(self.n_params, np.float32)
+        loss = C.c_float()
+        _check(lib().hx_mlp_gradients(self._h, _p(x), _p(t), x.shape[0], C.byref(loss), _p(g), self.n_params))
+        return float(loss.value), g
+
+    def train(self, x: np.ndarray, t: np.ndarray, batch: int, iters: int, lr: float, seed: int = 0) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        trace = np.zeros(iters, np.float32)
+        _check(lib().hx_mlp_train(self._h, _p(x), _p(t), x.shape[0], batch, iters, lr, seed, _p(trace)))
+        return trace
+
+
+class Closure:
+    """Learned closure of a truncated hierarchy (wraps hx_closure)."""
+
+    def __init__(self, coarse_problem, fine_max_depth: int, hidden: int = 512, capacity: int = 64, seed: int = 0):
+        prob, self._keep = _problem_struct(coarse_problem)
+        h = C.c_void_p()
+        _check(lib().hx_closure_create(C.byref(prob), fine_max_depth, hidden, capacity, seed, C.byref(h)))
+        self._h = h
+        m = C.c_void_p()
+        _check(lib().hx_closure_mlp(self._h, C.byref(m)))
+        d2 = coarse_problem.dim ** 2
+        self.mlp = MLP(2 * d2 + coarse_problem.modes, hidden, 2 * d2, handle=m, owner=self)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().hx_closure_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        si, so = C.c_double(), C.c_double()
+        _check(lib().hx_closure_info(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(si), C.byref(so)))
+        return {"top_ados": a.value, "up_ados": b.value, "snapshots": c.value, "s_in": si.value, "s_out": so.value}
+
+    def harvest(self, fine_ctx) -> None:
+        _check(lib().hx_closure_harvest(self._h, fine_ctx._h))
+
+    def train(self, iters: int, batch: int = 1024, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+        trace = np.zeros(iters, np.float32)
+        _check(lib().hx_closure_train(self._h, iters, batch, lr, seed, _p(trace)))
+        return trace
+
+    def set_scales(self, s_in: float, s_out: float) -> None:
+        _check(lib().hx_closure_set_scales(self._h, s_in, s_out))
+
+    def attach(self, ctx) -> None:
+        _check(lib().hx_ctx_set_closure(ctx._h, self._h))

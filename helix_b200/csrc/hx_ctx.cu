@@ -227,10 +227,23 @@ int launch_large_stage(hx_ctx* c, const double2* u, const double2* rho, double2*
     return k + 1;
 }
 
+int launch_stage_core(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base);
+
+// One stage, then the learned closure term when one is attached.
+int launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
+{
+    int k = launch_stage_core(c, u, rho, out, alpha, base);
+    if (c->closure) {
+        hx::closure_stage(c->closure, c, u, out, alpha, c->stream);
+        k += 5;  // input rows, three GEMMs, closure add
+    }
+    return k;
+}
+
 // One stage: the two-pass flip path when V has spin-flip parts or d > 64; for
 // d = 32, 64 the up-term kernel of tier L-1 followed by the fused multi-CTA
 // kernel; the generic kernel otherwise.  Returns kernels launched.
-int launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
+int launch_stage_core(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
 {
     if (c->use_large) return launch_large_stage(c, u, rho, out, alpha, base);
     if (c->use_flip) {
@@ -803,6 +816,21 @@ int hx_ctx_rhs(hx_ctx* c, double* out, uint64_t n)
     HX_CUDA_TRY(cudaMemcpyAsync(out, c->ua, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return read_error_flag(c);
+}
+
+int hx_ctx_set_closure(hx_ctx* c, hx_closure* cl)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
+    if (cl) {
+        uint32_t top = 0;
+        hx_closure_info(cl, &top, nullptr, nullptr, nullptr, nullptr);
+        if (c->mixed || c->use_flip || c->use_large || c->d > 64)
+            return fail(HX_ERR_UNSUPPORTED_EXECUTION, "closures run with double precision and dim <= 64");
+        if (!hx::closure_matches_hierarchy(cl, c->d, c->M, c->H))
+            return fail(HX_ERR_INVALID_RUNTIME_OPTION, "the closure was made for another hierarchy");
+    }
+    c->closure = cl;
+    return HX_OK;
 }
 
 int hx_ctx_check_finite(hx_ctx* c)

@@ -180,6 +180,12 @@ void launch_ado0(const Ado0Args& a, const double2* u0, const float2* u, const do
 void launch_d2f(const double2* in, float2* out, long long n, cudaStream_t s);
 void launch_vec_d2f(const double* in, float* out, long long n, cudaStream_t s);
 
+// Whether a closure was made for a hierarchy of this dimension, mode count and size (hx_mlp.cu)
+bool closure_matches_hierarchy(const ::hx_closure* cl, int d, int M, long long H);
+// Learned closure term of a stage: out_top += alpha * (dropped up coupling) (hx_mlp.cu)
+int closure_stage(::hx_closure* cl, const ::hx_ctx* c, const double2* u, double2* out, double alpha,
+                  cudaStream_t s);
+
 // Argument blocks of a context's fused and up-term kernels (hx_ctx.cu)
 FusedArgs fused_args_of(const ::hx_ctx* c);
 UpTermArgs upterm_args_of(const ::hx_ctx* c);
@@ -250,6 +256,7 @@ struct hx_ctx {
     bool use_flip = false;        // two-pass flip path (flips in V, or d > 1024)
     bool use_large = false;       // band kernels for 128 <= d <= 1024, diagonal V (hx_large.cu)
     bool mixed = false;           // complex64 hierarchy, ADO 0 in double precision
+    hx_closure* closure = nullptr; // learned closure term added by every stage (hx_mlp.cu)
     float2* rho32 = nullptr;      // mixed: complex64 state buffers (rho, ua, ub mirror them)
     float2* ua32 = nullptr;
     float2* ub32 = nullptr;

@@ -1,0 +1,935 @@
+// Learned closure of the hierarchy: a small MLP in BF16 with FP32
+// accumulation, its training kernels, and its use inside the propagator.
+//
+// Network: x (the 2 d^2 reals of an ADO of the top tier, scaled, and a
+// one-hot mode index) -> Linear(in, hidden) -> GELU -> Linear(hidden, hidden)
+// -> GELU -> Linear(hidden, 2 d^2) = the scaled prediction of its up
+// neighbour in the next tier, which the truncated hierarchy drops.  Weights
+// are kept in FP32 (Adam master copy) and used in BF16 by the GEMMs.
+//
+// GEMM: C = op(A) op(B), BF16 operands, FP32 accumulation on the tensor cores
+// (WMMA 16x16x16 fragments), 64x64 tiles staged in shared memory, fused
+// epilogues (bias + GELU keeping the pre-activation, bias, plain, GELU
+// backward).  Training: MSE loss, backward pass, Adam, all on the device.
+// The training set lives on the device: harvest kernels copy, from a deep
+// (fine) hierarchy's state, the top-tier ADOs of the truncated (coarse)
+// hierarchy and their up neighbours.
+//
+// No counterpart in the reference, which truncates the hierarchy at
+// Param::JMax (src/parameters.cu:31, src/initialize_detail.h:196-213).
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <mma.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "hx_internal.h"
+
+using hx::fail;
+using bf16 = __nv_bfloat16;
+
+namespace hx {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 32, GT = 128;
+
+enum Epi : int { kEpiBiasGelu = 0, kEpiBias = 1, kEpiStore = 2, kEpiGeluBack = 3 };
+
+struct GemmOut {
+    const float* bias;   // [N]
+    float* outf;         // FP32 result (pre-activation for kEpiBiasGelu)
+    bf16* outh;          // BF16 result (GELU output, or dZ for kEpiGeluBack)
+    const float* aux;    // pre-activation Z for kEpiGeluBack
+    int ldo;
+};
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+
+__device__ __forceinline__ float gelu_grad(float z)
+{
+    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+    return cdf + z * pdf;
+}
+
+// C[M x N] = op(A) op(B); op(A) = A (row-major M x K, lda) or A^T (A stored K x M);
+// op(B) = B (row-major K x N, ldb) or B^T (B stored N x K).  Four warps, each a 32 x 32 block.
+template <bool TA, bool TB, int EPI>
+__global__ void __launch_bounds__(GT)
+    gemm_kernel(int M, int N, int K, const bf16* __restrict__ A, int lda, const bf16* __restrict__ B, int ldb,
+                GemmOut o)
+{
+    using namespace nvcuda;
+    __shared__ __align__(32) bf16 sA[BM][BK + 8];
+    __shared__ __align__(32) bf16 sB[BK][BN + 8];
+    __shared__ __align__(32) float sC[BM][BN + 4];
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int warp = threadIdx.x >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[2][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) wmma::fill_fragment(acc[i][j], 0.0f);
+    const bf16 zero = __float2bfloat16(0.0f);
+    for (int k0 = 0; k0 < K; k0 += BK) {
+        for (int idx = threadIdx.x; idx < BM * BK; idx += GT) {
+            int mm, kk;
+            if (!TA) {
+                mm = idx / BK;
+                kk = idx % BK;
+            } else {
+                kk = idx / BM;
+                mm = idx % BM;
+            }
+            const int gm = m0 + mm, gk = k0 + kk;
+            bf16 v = zero;
+            if (gm < M && gk < K)
+                v = TA ? A[static_cast<long long>(gk) * lda + gm] : A[static_cast<long long>(gm) * lda + gk];
+            sA[mm][kk] = v;
+        }
+        for (int idx = threadIdx.x; idx < BK * BN; idx += GT) {
+            int kk, nn;
+            if (!TB) {
+                kk = idx / BN;
+                nn = idx % BN;
+            } else {
+                nn = idx / BK;
+                kk = idx % BK;
+            }
+            const int gn = n0 + nn, gk = k0 + kk;
+            bf16 v = zero;
+            if (gn < N && gk < K)
+                v = TB ? B[static_cast<long long>(gn) * ldb + gk] : B[static_cast<long long>(gk) * ldb + gn];
+            sB[kk][nn] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 16) {
+            wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> fa[2];
+            wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> fb[2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) wmma::load_matrix_sync(fa[i], &sA[wm + 16 * i][kk], BK + 8);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) wmma::load_matrix_sync(fb[j], &sB[kk][wn + 16 * j], BN + 8);
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) wmma::mma_sync(acc[i][j], fa[i], fb[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+            wmma::store_matrix_sync(&sC[wm + 16 * i][wn + 16 * j], acc[i][j], BN + 4, wmma::mem_row_major);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < BM * BN; idx += GT) {
+        const int mm = idx / BN, nn = idx % BN;
+        const int gm = m0 + mm, gn = n0 + nn;
+        if (gm >= M || gn >= N) continue;
+        const float v = sC[mm][nn];
+        const long long off = static_cast<long long>(gm) * o.ldo + gn;
+        if (EPI == kEpiBiasGelu) {
+            const float z = v + o.bias[gn];
+            o.outf[off] = z;
+            o.outh[off] = __float2bfloat16(gelu(z));
+        } else if (EPI == kEpiBias) {
+            o.outf[off] = v + o.bias[gn];
+        } else if (EPI == kEpiStore) {
+            o.outf[off] = v;
+        } else {
+            o.outh[off] = __float2bfloat16(v * gelu_grad(o.aux[off]));
+            if (o.outf) o.outf[off] = v * gelu_grad(o.aux[off]);
+        }
+    }
+}
+
+template <bool TA, bool TB, int EPI>
+void gemm(int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb, const GemmOut& o, cudaStream_t s)
+{
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    gemm_kernel<TA, TB, EPI><<<grid, GT, 0, s>>>(M, N, K, A, lda, B, ldb, o);
+}
+
+// column sums of an FP32 matrix [rows x cols] (bias gradients); fixed order
+__global__ void colsum_kernel(const float* __restrict__ x, int rows, int cols, int ld, float* out)
+{
+    const int cidx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cidx >= cols) return;
+    float s = 0.f;
+    for (int r = 0; r < rows; ++r) s += x[static_cast<long long>(r) * ld + cidx];
+    out[cidx] = s;
+}
+
+// residual R = Y - T, dY = 2 R / (rows cols) (FP32 and BF16); per-block partial sums of R^2
+__global__ void mse_kernel(const float* __restrict__ y, const float* __restrict__ t, long long n, float scale,
+                           float* dyf, bf16* dyh, float* partial)
+{
+    float s = 0.f;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const float r = y[i] - t[i];
+        s += r * r;
+        const float g = scale * r;
+        dyf[i] = g;
+        dyh[i] = __float2bfloat16(g);
+    }
+    __shared__ float red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+__global__ void adam_kernel(float* w, const float* g, float* m, float* v, bf16* wh, long long n, float lr, float b1,
+                            float b2, float c1, float c2, float eps)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        w[i] = wi;
+        wh[i] = __float2bfloat16(wi);
+    }
+}
+
+__global__ void f2h_kernel(const float* __restrict__ x, bf16* y, long long n)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+        y[i] = __float2bfloat16(x[i]);
+}
+
+// rows of X (BF16, ld = in_ld) from FP32 host-provided inputs [rows x in_dim]
+__global__ void pack_rows_kernel(const float* __restrict__ x, int rows, int in_dim, int in_ld, bf16* X)
+{
+    const long long n = static_cast<long long>(rows) * in_ld;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int r = static_cast<int>(i / in_ld), c = static_cast<int>(i % in_ld);
+        X[i] = __float2bfloat16(c < in_dim ? x[static_cast<long long>(r) * in_dim + c] : 0.f);
+    }
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Minibatch from a host-style dataset on the device: sample b = uniform row of (x, t).
+__global__ void gather_rows_kernel(const float* __restrict__ x, const float* __restrict__ t, int n, int in_dim,
+                                   int out_dim, int in_ld, int batch, uint64_t seed, bf16* X, float* T)
+{
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    const int row = static_cast<int>(mix64(seed ^ (0x5851F42D4C957F2Dull * (b + 1))) % static_cast<uint64_t>(n));
+    for (int c = threadIdx.x; c < in_ld; c += blockDim.x)
+        X[static_cast<long long>(b) * in_ld + c] =
+            __float2bfloat16(c < in_dim ? x[static_cast<long long>(row) * in_dim + c] : 0.f);
+    for (int c = threadIdx.x; c < out_dim; c += blockDim.x)
+        T[static_cast<long long>(b) * out_dim + c] = t[static_cast<long long>(row) * out_dim + c];
+}
+
+// Minibatch from the closure dataset: sample b = (snapshot, top-tier ADO i, mode k);
+// X row = [slab of ADO i / s_in (2 d^2 reals), one-hot k, 0...], T row = up neighbour / s_out.
+__global__ void gather_closure_kernel(const float2* __restrict__ din, const float2* __restrict__ dout,
+                                      const int* __restrict__ up_local, int n_snap, int n_top, int n_up, int M,
+                                      int d2, float inv_in, float inv_out, int in_ld, int batch, uint64_t seed,
+                                      bf16* X, float* T)
+{
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    const uint64_t r = mix64(seed ^ (0x2545F4914F6CDD1Dull * (b + 1)));
+    const long long pairs = static_cast<long long>(n_snap) * n_top * M;
+    const long long pidx = static_cast<long long>(r % static_cast<uint64_t>(pairs));
+    const int snap = static_cast<int>(pidx / (static_cast<long long>(n_top) * M));
+    const int i = static_cast<int>((pidx / M) % n_top);
+    const int k = static_cast<int>(pidx % M);
+    const int t = up_local[i * M + k];
+    const float2* xi = din + (static_cast<long long>(snap) * n_top + i) * d2;
+    const float2* ti = dout + (static_cast<long long>(snap) * n_up + t) * d2;
+    bf16* Xb = X + static_cast<long long>(b) * in_ld;
+    float* Tb = T + static_cast<long long>(b) * 2 * d2;
+    for (int e = threadIdx.x; e < d2; e += blockDim.x) {
+        const float2 v = xi[e];
+        Xb[2 * e] = __float2bfloat16(v.x * inv_in);
+        Xb[2 * e + 1] = __float2bfloat16(v.y * inv_in);
+        const float2 w = ti[e];
+        Tb[2 * e] = w.x * inv_out;
+        Tb[2 * e + 1] = w.y * inv_out;
+    }
+    for (int c = 2 * d2 + threadIdx.x; c < in_ld; c += blockDim.x)
+        Xb[c] = __float2bfloat16(c - 2 * d2 == k ? 1.f : 0.f);
+}
+
+// Copy, from a fine hierarchy's state, the coarse top-tier ADOs and their up neighbours (FP32).
+__global__ void harvest_kernel(const double2* __restrict__ fine, const int* __restrict__ top_fine,
+                               const int* __restrict__ up_fine, int n_top, int n_up, int d2, float2* din,
+                               float2* dout)
+{
+    const int s = blockIdx.y;  // slab number: [0, n_top) top tier, then [0, n_up) up neighbours
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= d2) return;
+    if (s < n_top) {
+        const double2 v = fine[static_cast<long long>(top_fine[s]) * d2 + e];
+        din[static_cast<long long>(s) * d2 + e] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+    } else {
+        const int t = s - n_top;
+        const double2 v = fine[static_cast<long long>(up_fine[t]) * d2 + e];
+        dout[static_cast<long long>(t) * d2 + e] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+    }
+}
+
+// Closure input rows from the coarse state u: row (i, k) = [u_{top i} / s_in, one-hot k].
+__global__ void closure_input_kernel(const double2* __restrict__ u, const int* __restrict__ top, int n_top, int M,
+                                     int d2, float inv_in, int in_ld, bf16* X)
+{
+    const int row = blockIdx.x;  // i * M + k
+    const int i = row / M, k = row % M;
+    const double2* ui = u + static_cast<long long>(top[i]) * d2;
+    bf16* Xb = X + static_cast<long long>(row) * in_ld;
+    for (int e = threadIdx.x; e < d2; e += blockDim.x) {
+        const double2 v = ui[e];
+        Xb[2 * e] = __float2bfloat16(static_cast<float>(v.x) * inv_in);
+        Xb[2 * e + 1] = __float2bfloat16(static_cast<float>(v.y) * inv_in);
+    }
+    for (int c = 2 * d2 + threadIdx.x; c < in_ld; c += blockDim.x)
+        Xb[c] = __float2bfloat16(c - 2 * d2 == k ? 1.f : 0.f);
+}
+
+// out_{top i} += alpha sum_k -i (v_{j(k)}(r) - v_{j(k)}(c)) (s_out Y_{i,k})   (the dropped up coupling)
+__global__ void closure_add_kernel(const float* __restrict__ Y, const int* __restrict__ top,
+                                   const int* __restrict__ mode_bath, const double* __restrict__ vdiag, int n_top,
+                                   int M, int logd, double s_out, double alpha, double2* out)
+{
+    const int D = 1 << logd;
+    const int d2 = D * D;
+    const int i = blockIdx.y;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= d2 || i >= n_top) return;
+    const int r = e >> logd, c = e & (D - 1);
+    double sr = 0.0, si = 0.0;
+    for (int k = 0; k < M; ++k) {
+        const int j = mode_bath[k];
+        const double del = vdiag[j * D + r] - vdiag[j * D + c];
+        if (del == 0.0) continue;
+        const float* y = Y + (static_cast<long long>(i) * M + k) * 2 * d2;
+        sr += del * y[2 * e];
+        si += del * y[2 * e + 1];
+    }
+    // -i del Y = del (Y.y - i Y.x)
+    double2* o = out + static_cast<long long>(top[i]) * d2 + e;
+    o->x += alpha * s_out * si;
+    o->y -= alpha * s_out * sr;
+}
+
+// sum of squares of FP32 complex data (deterministic two-level sum)
+__global__ void sumsq_kernel(const float2* __restrict__ x, long long n, double* partial)
+{
+    double s = 0.0;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+        s += static_cast<double>(x[i].x) * x[i].x + static_cast<double>(x[i].y) * x[i].y;
+    __shared__ double red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+}  // namespace
+
+}  // namespace hx
+
+// ---------------------------------------------------------------------------
+// MLP object
+// ---------------------------------------------------------------------------
+
+struct hx_mlp {
+    int in_dim = 0, in_ld = 0, hidden = 0, out_dim = 0;
+    long long n_params = 0;
+    cudaStream_t stream = nullptr;
+    // FP32 parameters (W1 b1 W2 b2 W3 b3, contiguous), gradients, Adam moments, BF16 copy
+    float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    bf16* wh = nullptr;
+    long long adam_t = 0;
+    // activations for one batch
+    int cap = 0;
+    bf16 *X = nullptr, *H1 = nullptr, *H2 = nullptr, *dYh = nullptr, *dZ2h = nullptr, *dZ1h = nullptr;
+    float *Z1 = nullptr, *Z2 = nullptr, *Y = nullptr, *T = nullptr, *dYf = nullptr, *dZ2f = nullptr, *dZ1f = nullptr;
+    float* partial = nullptr;
+    float* pinned = nullptr;
+    // parameter offsets
+    long long oW1 = 0, ob1 = 0, oW2 = 0, ob2 = 0, oW3 = 0, ob3 = 0;
+};
+
+namespace {
+
+void mlp_free_batch(hx_mlp* n)
+{
+    void* p[] = {n->X, n->H1, n->H2, n->dYh, n->dZ2h, n->dZ1h, n->Z1, n->Z2, n->Y, n->T, n->dYf, n->dZ2f, n->dZ1f};
+    for (void* q : p)
+        if (q) cudaFree(q);
+    n->X = n->H1 = n->H2 = n->dYh = n->dZ2h = n->dZ1h = nullptr;
+    n->Z1 = n->Z2 = n->Y = n->T = n->dYf = n->dZ2f = n->dZ1f = nullptr;
+    n->cap = 0;
+}
+
+int mlp_reserve(hx_mlp* n, int batch)
+{
+    if (batch <= n->cap) return HX_OK;
+    mlp_free_batch(n);
+    const size_t B = static_cast<size_t>(batch);
+    cudaError_t e = cudaMalloc(&n->X, B * n->in_ld * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc(&n->H1, B * n->hidden * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc(&n->H2, B * n->hidden * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc(&n->dYh, B * n->out_dim * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc(&n->dZ2h, B * n->hidden * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc(&n->dZ1h, B * n->hidden * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc(&n->Z1, B * n->hidden * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->Z2, B * n->hidden * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->Y, B * n->out_dim * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->T, B * n->out_dim * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->dYf, B * n->out_dim * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->dZ2f, B * n->hidden * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->dZ1f, B * n->hidden * sizeof(float));
+    if (e != cudaSuccess) {
+        mlp_free_batch(n);
+        return hx::cuda_fail(e, "cudaMalloc (MLP activations)");
+    }
+    n->cap = batch;
+    return HX_OK;
+}
+
+// Forward pass of rows X[0..B) (BF16, already in n->X): Z1, H1, Z2, H2, Y.
+void mlp_forward(hx_mlp* n, int B, cudaStream_t s)
+{
+    using namespace hx;
+    const bf16* W = n->wh;
+    gemm<false, true, kEpiBiasGelu>(B, n->hidden, n->in_dim, n->X, n->in_ld, W + n->oW1, n->in_dim,
+                                    GemmOut{n->w + n->ob1, n->Z1, n->H1, nullptr, n->hidden}, s);
+    gemm<false, true, kEpiBiasGelu>(B, n->hidden, n->hidden, n->H1, n->hidden, W + n->oW2, n->hidden,
+                                    GemmOut{n->w + n->ob2, n->Z2, n->H2, nullptr, n->hidden}, s);
+    gemm<false, true, kEpiBias>(B, n->out_dim, n->hidden, n->H2, n->hidden, W + n->oW3, n->hidden,
+                                GemmOut{n->w + n->ob3, n->Y, nullptr, nullptr, n->out_dim}, s);
+}
+
+// MSE loss against n->T and the gradient of every parameter into n->g; returns the loss.
+int mlp_backward(hx_mlp* n, int B, float* loss, cudaStream_t s)
+{
+    using namespace hx;
+    const long long ny = static_cast<long long>(B) * n->out_dim;
+    const int nb = 148;
+    mse_kernel<<<nb, 256, 0, s>>>(n->Y, n->T, ny, 2.0f / static_cast<float>(ny), n->dYf, n->dYh, n->partial);
+    const bf16* W = n->wh;
+    // layer 3
+    gemm<true, false, kEpiStore>(n->out_dim, n->hidden, B, n->dYh, n->out_dim, n->H2, n->hidden,
+                                 GemmOut{nullptr, n->g + n->oW3, nullptr, nullptr, n->hidden}, s);
+    colsum_kernel<<<(n->out_dim + 255) / 256, 256, 0, s>>>(n->dYf, B, n->out_dim, n->out_dim, n->g + n->ob3);
+    gemm<false, false, kEpiGeluBack>(B, n->hidden, n->out_dim, n->dYh, n->out_dim, W + n->oW3, n->hidden,
+                                     GemmOut{nullptr, n->dZ2f, n->dZ2h, n->Z2, n->hidden}, s);
+    // layer 2
+    gemm<true, false, kEpiStore>(n->hidden, n->hidden, B, n->dZ2h, n->hidden, n->H1, n->hidden,
+                                 GemmOut{nullptr, n->g + n->oW2, nullptr, nullptr, n->hidden}, s);
+    colsum_kernel<<<(n->hidden + 255) / 256, 256, 0, s>>>(n->dZ2f, B, n->hidden, n->hidden, n->g + n->ob2);
+    gemm<false, false, kEpiGeluBack>(B, n->hidden, n->hidden, n->dZ2h, n->hidden, W + n->oW2, n->hidden,
+                                     GemmOut{nullptr, n->dZ1f, n->dZ1h, n->Z1, n->hidden}, s);
+    // layer 1
+    gemm<true, false, kEpiStore>(n->hidden, n->in_dim, B, n->dZ1h, n->hidden, n->X, n->in_ld,
+                                 GemmOut{nullptr, n->g + n->oW1, nullptr, nullptr, n->in_dim}, s);
+    colsum_kernel<<<(n->hidden + 255) / 256, 256, 0, s>>>(n->dZ1f, B, n->hidden, n->hidden, n->g + n->ob1);
+    if (loss) {
+        HX_CUDA_TRY(cudaMemcpyAsync(n->pinned, n->partial, nb * sizeof(float), cudaMemcpyDeviceToHost, s));
+        HX_CUDA_TRY(cudaStreamSynchronize(s));
+        double acc = 0.0;
+        for (int i = 0; i < nb; ++i) acc += n->pinned[i];
+        *loss = static_cast<float>(acc / static_cast<double>(ny));
+    }
+    return HX_OK;
+}
+
+void mlp_adam(hx_mlp* n, float lr, cudaStream_t s)
+{
+    n->adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, static_cast<float>(n->adam_t));
+    const float c2 = 1.f - std::pow(b2, static_cast<float>(n->adam_t));
+    hx::adam_kernel<<<148 * 4, 256, 0, s>>>(n->w, n->g, n->m, n->v, n->wh, n->n_params, lr, b1, b2, c1, c2, 1e-8f);
+}
+
+void mlp_release(hx_mlp* n)
+{
+    if (!n) return;
+    if (n->stream) cudaStreamSynchronize(n->stream);
+    mlp_free_batch(n);
+    void* p[] = {n->w, n->g, n->m, n->v, n->wh, n->partial};
+    for (void* q : p)
+        if (q) cudaFree(q);
+    if (n->pinned) cudaFreeHost(n->pinned);
+    if (n->stream) cudaStreamDestroy(n->stream);
+    delete n;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Closure object: index maps, device training set, the MLP
+// ---------------------------------------------------------------------------
+
+struct hx_closure {
+    hx_mlp* net = nullptr;
+    int d = 0, logd = 0, d2 = 0, M = 0, J = 0;
+    uint32_t coarse_depth = 0, fine_depth = 0;
+    int n_top = 0, n_up = 0;
+    std::vector<int> mode_bath;
+    int* top_coarse = nullptr;   // [n_top] coarse index of each top-tier ADO
+    int* top_fine = nullptr;     // [n_top] its index in the fine hierarchy
+    int* up_fine = nullptr;      // [n_up] fine index of each distinct up neighbour
+    int* up_local = nullptr;     // [n_top][M] which of them is n_top[i] + e_k
+    int* mode_bath_d = nullptr;  // [M]
+    float2* din = nullptr;       // [cap][n_top][d2]
+    float2* dout = nullptr;      // [cap][n_up][d2]
+    int cap = 0, n_snap = 0;
+    double s_in = 1.0, s_out = 1.0;  // RMS scales of inputs and targets
+    bool scaled = false;
+    cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+void closure_release(hx_closure* c)
+{
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void* p[] = {c->top_coarse, c->top_fine, c->up_fine, c->up_local, c->mode_bath_d, c->din, c->dout};
+    for (void* q : p)
+        if (q) cudaFree(q);
+    if (c->net) mlp_release(c->net);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+double rms_of(const float2* x, long long n, cudaStream_t s)
+{
+    double* partial = nullptr;
+    if (cudaMalloc(&partial, 148 * sizeof(double)) != cudaSuccess) return -1.0;
+    hx::sumsq_kernel<<<148, 256, 0, s>>>(x, n, partial);
+    double h[148];
+    cudaMemcpyAsync(h, partial, sizeof(h), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    cudaFree(partial);
+    double acc = 0.0;
+    for (double v : h) acc += v;
+    return std::sqrt(acc / (2.0 * static_cast<double>(n)));
+}
+
+}  // namespace
+
+// closure hook used by the context's stages (hx_ctx.cu)
+bool hx::closure_matches_hierarchy(const hx_closure* cl, int d, int M, long long H)
+{
+    uint64_t Hc = 0;
+    hx_hierarchy_size(static_cast<uint32_t>(cl->M), cl->coarse_depth, &Hc);
+    return cl->d == d && cl->M == M && static_cast<long long>(Hc) == H;
+}
+
+namespace hx {
+int closure_stage(hx_closure* cl, const ::hx_ctx* c, const double2* u, double2* out, double alpha, cudaStream_t s)
+{
+    if (!cl || !cl->scaled) return HX_OK;
+    const int rows = cl->n_top * cl->M;
+    hx_mlp* n = cl->net;
+    int rc = mlp_reserve(n, rows);
+    if (rc != HX_OK) return rc;
+    closure_input_kernel<<<rows, 256, 0, s>>>(u, cl->top_coarse, cl->n_top, cl->M, cl->d2,
+                                              static_cast<float>(1.0 / cl->s_in), n->in_ld, n->X);
+    mlp_forward(n, rows, s);
+    dim3 grid((cl->d2 + 255) / 256, cl->n_top);
+    closure_add_kernel<<<grid, 256, 0, s>>>(n->Y, cl->top_coarse, cl->mode_bath_d, c->vdiag, cl->n_top, cl->M,
+                                           cl->logd, cl->s_out, alpha, out);
+    return HX_OK;
+}
+}  // namespace hx
+
+extern "C" {
+
+int hx_mlp_create(uint32_t in_dim, uint32_t hidden, uint32_t out_dim, uint64_t seed, hx_mlp** out)
+{
+    if (!out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL MLP output");
+    *out = nullptr;
+    if (in_dim == 0 || hidden == 0 || out_dim == 0 || in_dim > 65536 || hidden > 8192 || out_dim > 65536)
+        return fail(HX_ERR_INVALID_RUNTIME_OPTION, "MLP dimensions out of range");
+    hx_mlp* n = new (std::nothrow) hx_mlp();
+    if (!n) return fail(HX_ERR_OUT_OF_MEMORY, "host allocation failed");
+    n->in_dim = static_cast<int>(in_dim);
+    n->in_ld = (n->in_dim + 7) & ~7;
+    n->hidden = static_cast<int>(hidden);
+    n->out_dim = static_cast<int>(out_dim);
+    n->oW1 = 0;
+    n->ob1 = n->oW1 + static_cast<long long>(hidden) * in_dim;
+    n->oW2 = n->ob1 + hidden;
+    n->ob2 = n->oW2 + static_cast<long long>(hidden) * hidden;
+    n->oW3 = n->ob2 + hidden;
+    n->ob3 = n->oW3 + static_cast<long long>(out_dim) * hidden;
+    n->n_params = n->ob3 + out_dim;
+    // the BF16 copies of W2, W3 start at offsets oW2, oW3: keep them 16-byte aligned
+    auto bail = [&](int rc) {
+        mlp_release(n);
+        return rc;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking);
+    const size_t np = static_cast<size_t>(n->n_params);
+    if (e == cudaSuccess) e = cudaMalloc(&n->w, np * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->g, np * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->m, np * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->v, np * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->wh, np * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc(&n->partial, 256 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMallocHost(&n->pinned, 256 * sizeof(float));
+    if (e != cudaSuccess) return bail(hx::cuda_fail(e, "cudaMalloc (MLP)"));
+    // He-style uniform init from splitmix64(seed), biases zero
+    std::vector<float> w(np, 0.f);
+    uint64_t st = seed;
+    auto uni = [&]() {
+        st += 0x9E3779B97F4A7C15ull;
+        uint64_t z = st;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return static_cast<double>(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto fill = [&](long long off, long long count, int fan_in) {
+        const double a = std::sqrt(6.0 / fan_in);
+        for (long long i = 0; i < count; ++i) w[off + i] = static_cast<float>((2.0 * uni() - 1.0) * a);
+    };
+    fill(n->oW1, static_cast<long long>(hidden) * in_dim, static_cast<int>(in_dim));
+    fill(n->oW2, static_cast<long long>(hidden) * hidden, static_cast<int>(hidden));
+    fill(n->oW3, static_cast<long long>(out_dim) * hidden, static_cast<int>(hidden));
+    const int rc = hx_mlp_set_params(n, w.data(), np);
+    if (rc != HX_OK) return bail(rc);
+    *out = n;
+    return HX_OK;
+}
+
+void hx_mlp_destroy(hx_mlp* n) { mlp_release(n); }
+
+int hx_mlp_num_params(const hx_mlp* n, uint64_t* count)
+{
+    if (!n || !count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    *count = static_cast<uint64_t>(n->n_params);
+    return HX_OK;
+}
+
+int hx_mlp_set_params(hx_mlp* n, const float* params, uint64_t count)
+{
+    if (!n || !params) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    if (count != static_cast<uint64_t>(n->n_params)) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "parameter count mismatch");
+    const size_t np = static_cast<size_t>(n->n_params);
+    HX_CUDA_TRY(cudaMemcpyAsync(n->w, params, np * sizeof(float), cudaMemcpyHostToDevice, n->stream));
+    HX_CUDA_TRY(cudaMemsetAsync(n->m, 0, np * sizeof(float), n->stream));
+    HX_CUDA_TRY(cudaMemsetAsync(n->v, 0, np * sizeof(float), n->stream));
+    hx::f2h_kernel<<<148 * 4, 256, 0, n->stream>>>(n->w, n->wh, n->n_params);
+    HX_CUDA_TRY(cudaGetLastError());
+    HX_CUDA_TRY(cudaStreamSynchronize(n->stream));
+    n->adam_t = 0;
+    return HX_OK;
+}
+
+int hx_mlp_get_params(hx_mlp* n, float* params, uint64_t count)
+{
+    if (!n || !params) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    if (count != static_cast<uint64_t>(n->n_params)) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "parameter count mismatch");
+    HX_CUDA_TRY(cudaMemcpyAsync(params, n->w, n->n_params * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
+    HX_CUDA_TRY(cudaStreamSynchronize(n->stream));
+    return HX_OK;
+}
+
+int hx_mlp_forward(hx_mlp* n, const float* x, uint32_t rows, float* y)
+{
+    if (!n || !x || !y) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    if (rows == 0) return HX_OK;
+    int rc = mlp_reserve(n, static_cast<int>(rows));
+    if (rc != HX_OK) return rc;
+    float* dx = nullptr;
+    const size_t nx = static_cast<size_t>(rows) * n->in_dim;
+    HX_CUDA_TRY(cudaMalloc(&dx, nx * sizeof(float)));
+    cudaError_t e = cudaMemcpyAsync(dx, x, nx * sizeof(float), cudaMemcpyHostToDevice, n->stream);
+    if (e == cudaSuccess) {
+        hx::pack_rows_kernel<<<148 * 4, 256, 0, n->stream>>>(dx, static_cast<int>(rows), n->in_dim, n->in_ld, n->X);
+        mlp_forward(n, static_cast<int>(rows), n->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(y, n->Y, static_cast<size_t>(rows) * n->out_dim * sizeof(float), cudaMemcpyDeviceToHost,
+                            n->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(n->stream);
+    cudaFree(dx);
+    if (e != cudaSuccess) return hx::cuda_fail(e, "MLP forward");
+    return HX_OK;
+}
+
+int hx_mlp_gradients(hx_mlp* n, const float* x, const float* t, uint32_t rows, float* loss, float* grads,
+                     uint64_t count)
+{
+    if (!n || !x || !t || !grads) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    if (count != static_cast<uint64_t>(n->n_params)) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "parameter count mismatch");
+    if (rows == 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "empty batch");
+    int rc = mlp_reserve(n, static_cast<int>(rows));
+    if (rc != HX_OK) return rc;
+    float* dx = nullptr;
+    const size_t nx = static_cast<size_t>(rows) * n->in_dim, nt = static_cast<size_t>(rows) * n->out_dim;
+    HX_CUDA_TRY(cudaMalloc(&dx, nx * sizeof(float)));
+    cudaError_t e = cudaMemcpyAsync(dx, x, nx * sizeof(float), cudaMemcpyHostToDevice, n->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(n->T, t, nt * sizeof(float), cudaMemcpyHostToDevice, n->stream);
+    if (e == cudaSuccess) {
+        hx::pack_rows_kernel<<<148 * 4, 256, 0, n->stream>>>(dx, static_cast<int>(rows), n->in_dim, n->in_ld, n->X);
+        mlp_forward(n, static_cast<int>(rows), n->stream);
+        rc = mlp_backward(n, static_cast<int>(rows), loss, n->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && rc == HX_OK)
+        e = cudaMemcpyAsync(grads, n->g, n->n_params * sizeof(float), cudaMemcpyDeviceToHost, n->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(n->stream);
+    cudaFree(dx);
+    if (rc != HX_OK) return rc;
+    if (e != cudaSuccess) return hx::cuda_fail(e, "MLP gradients");
+    return HX_OK;
+}
+
+int hx_mlp_train(hx_mlp* n, const float* x, const float* t, uint32_t rows, uint32_t batch, uint32_t iters, float lr,
+                 uint64_t seed, float* loss_trace)
+{
+    if (!n || !x || !t) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    if (rows == 0 || batch == 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "empty data or batch");
+    int rc = mlp_reserve(n, static_cast<int>(batch));
+    if (rc != HX_OK) return rc;
+    float *dx = nullptr, *dt = nullptr;
+    const size_t nx = static_cast<size_t>(rows) * n->in_dim, nt = static_cast<size_t>(rows) * n->out_dim;
+    HX_CUDA_TRY(cudaMalloc(&dx, nx * sizeof(float)));
+    cudaError_t e = cudaMalloc(&dt, nt * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dx, x, nx * sizeof(float), cudaMemcpyHostToDevice, n->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, t, nt * sizeof(float), cudaMemcpyHostToDevice, n->stream);
+    for (uint32_t it = 0; it < iters && e == cudaSuccess && rc == HX_OK; ++it) {
+        hx::gather_rows_kernel<<<batch, 256, 0, n->stream>>>(dx, dt, static_cast<int>(rows), n->in_dim, n->out_dim,
+                                                            n->in_ld, static_cast<int>(batch), seed + it, n->X, n->T);
+        mlp_forward(n, static_cast<int>(batch), n->stream);
+        float l = 0.f;
+        rc = mlp_backward(n, static_cast<int>(batch), loss_trace ? &l : nullptr, n->stream);
+        if (loss_trace) loss_trace[it] = l;
+        mlp_adam(n, lr, n->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(n->stream);
+    cudaFree(dx);
+    cudaFree(dt);
+    if (rc != HX_OK) return rc;
+    if (e != cudaSuccess) return hx::cuda_fail(e, "MLP training");
+    return HX_OK;
+}
+
+int hx_closure_create(const hx_problem* coarse, uint32_t fine_max_depth, uint32_t hidden, uint32_t capacity,
+                      uint64_t seed, hx_closure** out)
+{
+    if (!out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL closure output");
+    *out = nullptr;
+    if (!coarse || !coarse->baths || coarse->n_baths == 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL problem");
+    const uint32_t d = coarse->dim;
+    if (d < 2 || d > 64 || (d & (d - 1)) != 0) return fail(HX_ERR_INVALID_DIMENSION, "closures need 2 <= dim <= 64");
+    if (coarse->max_depth < 2 || fine_max_depth <= coarse->max_depth)
+        return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "the fine hierarchy must be deeper than the coarse one (coarse max_depth >= 2)");
+    if (capacity == 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "capacity must be positive");
+    int M = 0;
+    std::vector<int> mb;
+    for (uint32_t j = 0; j < coarse->n_baths; ++j)
+        for (uint32_t k = 0; k <= coarse->baths[j].pade_terms; ++k, ++M) mb.push_back(static_cast<int>(j));
+    if (M > 128) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "too many modes");
+    uint64_t Hc = 0, Hf = 0;
+    int rc = hx_hierarchy_size(M, coarse->max_depth, &Hc);
+    if (rc == HX_OK) rc = hx_hierarchy_size(M, fine_max_depth, &Hf);
+    if (rc != HX_OK) return rc;
+    if (Hf >= (1ull << 31)) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "fine hierarchy too large");
+    std::vector<int32_t> rc_rows(Hc * M), rc_edges(Hc * 2 * M), rf_rows(Hf * M), rf_edges(Hf * 2 * M);
+    if ((rc = hx_hierarchy_tables(M, coarse->max_depth, rc_rows.data(), rc_edges.data(), Hc)) != HX_OK) return rc;
+    if ((rc = hx_hierarchy_tables(M, fine_max_depth, rf_rows.data(), rf_edges.data(), Hf)) != HX_OK) return rc;
+    // fine index of every index vector
+    std::map<std::vector<int32_t>, int> fine_of;
+    for (uint64_t i = 0; i < Hf; ++i)
+        fine_of[std::vector<int32_t>(rf_rows.begin() + i * M, rf_rows.begin() + (i + 1) * M)] = static_cast<int>(i);
+    hx_closure* c = new (std::nothrow) hx_closure();
+    if (!c) return fail(HX_ERR_OUT_OF_MEMORY, "host allocation failed");
+    auto bail = [&](int code) {
+        closure_release(c);
+        return code;
+    };
+    c->d = static_cast<int>(d);
+    while ((1 << c->logd) < c->d) ++c->logd;
+    c->d2 = c->d * c->d;
+    c->M = M;
+    c->J = static_cast<int>(coarse->n_baths);
+    c->coarse_depth = coarse->max_depth;
+    c->fine_depth = fine_max_depth;
+    c->mode_bath = mb;
+    // top tier of the coarse hierarchy and the fine indices of its up neighbours
+    std::vector<int> top_c, top_f, up_f, up_loc;
+    std::map<int, int> up_index;
+    for (uint64_t i = 0; i < Hc; ++i) {
+        std::vector<int32_t> v(rc_rows.begin() + i * M, rc_rows.begin() + (i + 1) * M);
+        int tier = 0;
+        for (int x : v) tier += x;
+        if (tier != static_cast<int>(coarse->max_depth) - 1) continue;
+        top_c.push_back(static_cast<int>(i));
+        top_f.push_back(fine_of.at(v));
+        for (int k = 0; k < M; ++k) {
+            std::vector<int32_t> w = v;
+            w[k] += 1;
+            const int fi = fine_of.at(w);
+            auto it = up_index.find(fi);
+            if (it == up_index.end()) {
+                it = up_index.emplace(fi, static_cast<int>(up_f.size())).first;
+                up_f.push_back(fi);
+            }
+            up_loc.push_back(it->second);
+        }
+    }
+    c->n_top = static_cast<int>(top_c.size());
+    c->n_up = static_cast<int>(up_f.size());
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    auto dalloc = [&](auto** p, size_t n) { return cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(**p)); };
+    if (e == cudaSuccess) e = dalloc(&c->top_coarse, top_c.size());
+    if (e == cudaSuccess) e = dalloc(&c->top_fine, top_f.size());
+    if (e == cudaSuccess) e = dalloc(&c->up_fine, up_f.size());
+    if (e == cudaSuccess) e = dalloc(&c->up_local, up_loc.size());
+    if (e == cudaSuccess) e = dalloc(&c->mode_bath_d, mb.size());
+    if (e == cudaSuccess) e = dalloc(&c->din, static_cast<size_t>(capacity) * c->n_top * c->d2);
+    if (e == cudaSuccess) e = dalloc(&c->dout, static_cast<size_t>(capacity) * c->n_up * c->d2);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->top_coarse, top_c.data(), top_c.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->top_fine, top_f.data(), top_f.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->up_fine, up_f.data(), up_f.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->up_local, up_loc.data(), up_loc.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->mode_bath_d, mb.data(), mb.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return bail(hx::cuda_fail(e, "closure set-up"));
+    c->cap = static_cast<int>(capacity);
+    if ((rc = hx_mlp_create(2 * c->d2 + M, hidden, 2 * c->d2, seed, &c->net)) != HX_OK) return bail(rc);
+    *out = c;
+    return HX_OK;
+}
+
+void hx_closure_destroy(hx_closure* c) { closure_release(c); }
+
+int hx_closure_mlp(hx_closure* c, hx_mlp** net)
+{
+    if (!c || !net) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    *net = c->net;
+    return HX_OK;
+}
+
+int hx_closure_info(const hx_closure* c, uint32_t* top_ados, uint32_t* up_ados, uint32_t* snapshots, double* s_in,
+                    double* s_out)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL closure");
+    if (top_ados) *top_ados = static_cast<uint32_t>(c->n_top);
+    if (up_ados) *up_ados = static_cast<uint32_t>(c->n_up);
+    if (snapshots) *snapshots = static_cast<uint32_t>(c->n_snap);
+    if (s_in) *s_in = c->s_in;
+    if (s_out) *s_out = c->s_out;
+    return HX_OK;
+}
+
+int hx_closure_harvest(hx_closure* c, hx_ctx* fine)
+{
+    if (!c || !fine) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    if (c->n_snap >= c->cap) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "closure training set is full");
+    hx_info info{};
+    int rc = hx_ctx_info(fine, &info);
+    if (rc != HX_OK) return rc;
+    uint64_t Hf = 0;
+    hx_hierarchy_size(c->M, c->fine_depth, &Hf);
+    if (static_cast<int>(info.dim) != c->d || static_cast<int>(info.modes) != c->M || info.hierarchy_size != Hf)
+        return fail(HX_ERR_INVALID_RUNTIME_OPTION, "the context is not the closure's fine hierarchy");
+    void* state = nullptr;
+    if ((rc = hx_ctx_state_device_ptr(fine, &state)) != HX_OK) return rc;
+    void* fs = nullptr;
+    if ((rc = hx_ctx_get_stream(fine, &fs)) != HX_OK) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(fs);
+    const long long snap = c->n_snap;
+    dim3 grid((c->d2 + 255) / 256, c->n_top + c->n_up);
+    hx::harvest_kernel<<<grid, 256, 0, s>>>(static_cast<const double2*>(state), c->top_fine, c->up_fine, c->n_top,
+                                           c->n_up, c->d2, c->din + snap * c->n_top * c->d2,
+                                           c->dout + snap * c->n_up * c->d2);
+    HX_CUDA_TRY(cudaGetLastError());
+    HX_CUDA_TRY(cudaStreamSynchronize(s));
+    c->n_snap += 1;
+    c->scaled = false;
+    return HX_OK;
+}
+
+int hx_closure_train(hx_closure* c, uint32_t iters, uint32_t batch, float lr, uint64_t seed, float* loss_trace)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL closure");
+    if (c->n_snap == 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "the closure training set is empty");
+    if (batch == 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "empty batch");
+    hx_mlp* n = c->net;
+    if (!c->scaled) {
+        const double si = rms_of(c->din, static_cast<long long>(c->n_snap) * c->n_top * c->d2, c->stream);
+        const double so = rms_of(c->dout, static_cast<long long>(c->n_snap) * c->n_up * c->d2, c->stream);
+        if (!(si > 0.0) || !(so > 0.0)) return fail(HX_ERR_NON_FINITE, "closure training data has no signal");
+        c->s_in = si;
+        c->s_out = so;
+        c->scaled = true;
+    }
+    int rc = mlp_reserve(n, static_cast<int>(batch));
+    if (rc != HX_OK) return rc;
+    // cosine learning-rate decay over the call
+    for (uint32_t it = 0; it < iters && rc == HX_OK; ++it) {
+        hx::gather_closure_kernel<<<batch, 256, 0, n->stream>>>(
+            c->din, c->dout, c->up_local, c->n_snap, c->n_top, c->n_up, c->M, c->d2,
+            static_cast<float>(1.0 / c->s_in), static_cast<float>(1.0 / c->s_out), n->in_ld, static_cast<int>(batch),
+            seed + it, n->X, n->T);
+        mlp_forward(n, static_cast<int>(batch), n->stream);
+        float l = 0.f;
+        rc = mlp_backward(n, static_cast<int>(batch), loss_trace ? &l : nullptr, n->stream);
+        if (loss_trace) loss_trace[it] = l;
+        const float f = 0.5f * (1.f + std::cos(3.14159265358979f * static_cast<float>(it) / static_cast<float>(iters)));
+        mlp_adam(n, lr * (0.05f + 0.95f * f), n->stream);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = hx::cuda_fail(e, "closure training");
+    }
+    if (rc != HX_OK) return rc;
+    HX_CUDA_TRY(cudaStreamSynchronize(n->stream));
+    return HX_OK;
+}
+
+int hx_closure_set_scales(hx_closure* c, double s_in, double s_out)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL closure");
+    if (!(s_in > 0.0) || !(s_out > 0.0)) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "scales must be positive");
+    c->s_in = s_in;
+    c->s_out = s_out;
+    c->scaled = true;
+    return HX_OK;
+}
+
+}  // extern "C"

@@ -258,6 +258,62 @@ int hx_batch_sync(hx_batch* batch);
 /* rho_0 of one instance (d*d complex, row-major) into a host buffer of n doubles. */
 int hx_batch_read_rho0(hx_batch* batch, uint32_t instance, double* out, uint64_t n);
 
+/* ------------------------------------------------------------------------
+ * Learned closure of a truncated hierarchy.  The reference truncates at
+ * Param::JMax and drops the next tier (src/parameters.cu:31,
+ * src/initialize_detail.h:196-213); a closure supplies, for every ADO n of the
+ * top tier and every mode k, a prediction of the dropped up neighbour
+ * rho_{n+e_k} from rho_n, by a small MLP (BF16 weights, FP32 accumulation)
+ * trained on the device from deeper (fine) hierarchies.  No counterpart in the
+ * reference.
+ * ------------------------------------------------------------------------ */
+typedef struct hx_mlp hx_mlp;
+
+/* in -> hidden -> GELU -> hidden -> GELU -> out; weights uniform(+-sqrt(6/fan_in))
+ * from splitmix64(seed), biases zero. */
+int hx_mlp_create(uint32_t in_dim, uint32_t hidden, uint32_t out_dim, uint64_t seed, hx_mlp** out);
+void hx_mlp_destroy(hx_mlp* mlp);
+/* Parameters as one FP32 array: W1 [hidden][in], b1, W2 [hidden][hidden], b2,
+ * W3 [out][hidden], b3.  Setting them resets the optimiser. */
+int hx_mlp_num_params(const hx_mlp* mlp, uint64_t* count);
+int hx_mlp_get_params(hx_mlp* mlp, float* params, uint64_t count);
+int hx_mlp_set_params(hx_mlp* mlp, const float* params, uint64_t count);
+/* y[rows][out] = MLP(x[rows][in]) (host buffers; x is rounded to BF16). */
+int hx_mlp_forward(hx_mlp* mlp, const float* x, uint32_t rows, float* y);
+/* Mean-squared-error loss of MLP(x) against t and its gradient with respect
+ * to every parameter (host buffers; layout as the parameters). */
+int hx_mlp_gradients(hx_mlp* mlp, const float* x, const float* t, uint32_t rows, float* loss, float* grads,
+                     uint64_t count);
+/* Adam (lr, 0.9, 0.999, 1e-8) on minibatches of `batch` rows drawn from
+ * (x, t) by splitmix64(seed + iteration); loss_trace[iters] may be NULL. */
+int hx_mlp_train(hx_mlp* mlp, const float* x, const float* t, uint32_t rows, uint32_t batch, uint32_t iters,
+                 float lr, uint64_t seed, float* loss_trace);
+
+typedef struct hx_closure hx_closure;
+
+/* Closure for the truncated (coarse) problem `coarse` (2 <= dim <= 64,
+ * max_depth >= 2), trained from fine hierarchies of the same system with
+ * max_depth = fine_max_depth; the training set holds up to `capacity`
+ * snapshots on the device; MLP width `hidden`. */
+int hx_closure_create(const hx_problem* coarse, uint32_t fine_max_depth, uint32_t hidden, uint32_t capacity,
+                      uint64_t seed, hx_closure** out);
+void hx_closure_destroy(hx_closure* closure);
+int hx_closure_mlp(hx_closure* closure, hx_mlp** mlp);
+int hx_closure_info(const hx_closure* closure, uint32_t* top_ados, uint32_t* up_ados, uint32_t* snapshots,
+                    double* s_in, double* s_out);
+/* Add one snapshot from the current state of a fine-hierarchy context: the
+ * coarse top-tier ADOs and their up neighbours. */
+int hx_closure_harvest(hx_closure* closure, hx_ctx* fine);
+/* Train on the snapshots (input and target scaled by their RMS over the set,
+ * fixed at the first call after a harvest; cosine-decayed Adam). */
+int hx_closure_train(hx_closure* closure, uint32_t iters, uint32_t batch, float lr, uint64_t seed,
+                     float* loss_trace);
+/* Scales of a closure whose parameters were set from elsewhere. */
+int hx_closure_set_scales(hx_closure* closure, double s_in, double s_out);
+/* Every stage of `ctx` (the coarse problem) adds the closure term; NULL
+ * detaches.  The closure must outlive its use. */
+int hx_ctx_set_closure(hx_ctx* ctx, hx_closure* closure);
+
 /* One evaluation of the right-hand side, drho = L(rho) for every ADO, that
  * allocates no memory.  No counterpart in the reference.
  *

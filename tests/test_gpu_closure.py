@@ -1,0 +1,102 @@
+"""GPU tests of the learned closure (hx_mlp.cu): the MLP's forward pass and
+gradients against the FP64 restatement with the same BF16 rounding points
+(oracle/mlp_oracle.py), training convergence, and the closure itself: a
+truncated hierarchy plus the trained network tracks the deep hierarchy's
+rho_0(t) better than the truncated hierarchy alone, on held-out seeds."""
+import numpy as np
+import pytest
+
+from helix_b200 import capi
+from helix_b200 import systems as S
+from oracle import mlp_oracle as MO
+
+pytestmark = pytest.mark.gpu
+
+
+def _trace_distance(a, b):
+    m = a - b
+    return 0.5 * float(np.sum(np.abs(np.linalg.eigvalsh(0.5 * (m + m.conj().T)))))
+
+
+def _net(i, h, o, seed):
+    net = capi.MLP(i, h, o, seed=seed)
+    rng = np.random.default_rng(seed)
+    p = (rng.standard_normal(net.n_params) * 0.2).astype(np.float32)
+    net.set_params(p)
+    return net, p
+
+
+def test_mlp_forward_and_gradients_match_oracle():
+    i, h, o, rows = 40, 64, 24, 32
+    net, p = _net(i, h, o, 5)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((rows, i)).astype(np.float32)
+    t = rng.standard_normal((rows, o)).astype(np.float32)
+    y = net.forward(x)
+    y_ref, loss_ref, g_ref = MO.forward_backward(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64),
+                                                 i, h, o, bf16=True)
+    assert np.max(np.abs(y - y_ref)) <= 1e-4 * max(1.0, np.max(np.abs(y_ref)))
+    loss, g = net.gradients(x, t)
+    assert abs(loss - loss_ref) <= 1e-4 * loss_ref
+    # FP32 accumulation and BF16 rounding of the back-propagated gradients:
+    # agreement to a few BF16 ulps of each block's scale
+    off = 0
+    for name, size in [("W1", h * i), ("b1", h), ("W2", h * h), ("b2", h), ("W3", o * h), ("b3", o)]:
+        gg, rr = g[off:off + size], g_ref[off:off + size]
+        scale = np.max(np.abs(rr))
+        assert np.max(np.abs(gg - rr)) <= 2e-2 * scale, name
+        assert np.corrcoef(gg, rr)[0, 1] > 0.9999, name
+        off += size
+
+
+def test_mlp_training_reduces_loss():
+    i, h, o = 32, 64, 16
+    rng = np.random.default_rng(2)
+    A = rng.standard_normal((o, i)) / np.sqrt(i)
+    x = rng.standard_normal((4096, i)).astype(np.float32)
+    t = (x @ A.T + 0.5 * np.tanh(x[:, :o])).astype(np.float32)
+    net = capi.MLP(i, h, o, seed=3)
+    trace = net.train(x, t, batch=256, iters=600, lr=3e-3, seed=9)
+    assert np.all(np.isfinite(trace))
+    assert trace[-50:].mean() < 0.1 * trace[:10].mean()
+
+
+def _rho_traj(problem, steps, closure=None):
+    with capi.Context(problem) as ctx:
+        if closure is not None:
+            closure.attach(ctx)
+        rho, _ = ctx.step_trace(steps, rho0=True, energy=False)
+    return rho
+
+
+def test_closure_beats_truncation_on_held_out_seeds():
+    n, K, steps, every = 3, 2, 300, 10
+    coarse_depth, fine_depth = 2, 5
+    train_seeds, test_seeds = [100 + s for s in range(6)], [900, 901]
+    coarse0 = S.spin_glass(n, seed=train_seeds[0], depth=coarse_depth, K=K, h=1.0, dt=0.01)
+    cl = capi.Closure(coarse0, fine_max_depth=fine_depth + 1, hidden=512, capacity=len(train_seeds) * steps // every)
+    for s in train_seeds:
+        fine = S.spin_glass(n, seed=s, depth=fine_depth, K=K, h=1.0, dt=0.01)
+        with capi.Context(fine) as ctx:
+            for _ in range(steps // every):
+                ctx.step(every)
+                cl.harvest(ctx)
+    info = cl.info()
+    assert info["snapshots"] == len(train_seeds) * steps // every
+    assert info["top_ados"] == 45 and info["up_ados"] > 0
+    trace = cl.train(iters=4000, batch=512, lr=1e-3, seed=4)
+    assert np.all(np.isfinite(trace)) and trace[-100:].mean() < 0.1 * trace[:20].mean()
+    gains = []
+    for s in test_seeds:
+        fine = S.spin_glass(n, seed=s, depth=fine_depth, K=K, h=1.0, dt=0.01)
+        coarse = S.spin_glass(n, seed=s, depth=coarse_depth, K=K, h=1.0, dt=0.01)
+        ref = _rho_traj(fine, steps)
+        plain = _rho_traj(coarse, steps)
+        closed = _rho_traj(coarse, steps, closure=cl)
+        e_plain = max(_trace_distance(plain[t], ref[t]) for t in range(0, steps, 20))
+        e_closed = max(_trace_distance(closed[t], ref[t]) for t in range(0, steps, 20))
+        gains.append(e_plain / e_closed)
+    # truncation at L=2 leaves a trace distance of ~2e-2 against L=5 here; the
+    # trained closure must cut it by a factor of 1.5 or more
+    assert min(gains) > 1.5, gains
+    cl.close()
