@@ -460,8 +460,20 @@ public:
         p.max_depth = static_cast<uint32_t>(hier.maxDepth);
         p.time_step = dt;
         p.integration_order = static_cast<uint32_t>(options_.integrationOrder);
-        p.precision = HX_PRECISION_DOUBLE;
-        const int rc = hx_ctx_create(&p, &ctx_);
+        // Single-precision requests take the mixed path (complex64 hierarchy,
+        // tier-0 ADO and observables in FP64) where it exists (128 <= d <= 1024,
+        // diagonal couplings, at least two tiers below the top), else FP64.
+        int rc = HX_ERR_UNSUPPORTED_PRECISION;
+        mixed_ = false;
+        if (options_.precision == Precision::Single) {
+            p.precision = HX_PRECISION_MIXED;
+            rc = hx_ctx_create(&p, &ctx_);
+            mixed_ = rc == HX_OK;
+        }
+        if (rc == HX_ERR_UNSUPPORTED_PRECISION) {
+            p.precision = HX_PRECISION_DOUBLE;
+            rc = hx_ctx_create(&p, &ctx_);
+        }
         if (rc != HX_OK) {
             lastCode_ = rc;
             throw std::runtime_error(hx_last_error());
@@ -522,6 +534,7 @@ public:
     const ContextOptions& options() const noexcept { return options_; }
     double dt() const noexcept { return dt_; }
     uint32_t dim() const noexcept { return dim_; }
+    bool mixed() const noexcept { return mixed_; }
     int lastCode() const noexcept { return lastCode_; }
 
 private:
@@ -543,6 +556,7 @@ private:
     hx_ctx* ctx_ = nullptr;
     double dt_ = 0.0;
     uint32_t dim_ = 0;
+    bool mixed_ = false;
     mutable int lastCode_ = HX_OK;
 };
 
@@ -660,8 +674,11 @@ RunResult HEOMSolver::run_steps(std::size_t steps)
             }
         }
         result.diagnostics.backend = copt.backend;
-        result.diagnostics.precision = Precision::Double;
-        if (copt.precision == Precision::Single)
+        result.diagnostics.precision = impl.mixed() ? Precision::Single : Precision::Double;
+        if (impl.mixed())
+            result.diagnostics.warnings.push_back(
+                "Precision::Single: hierarchy in complex64, tier-0 ADO and observables in double precision");
+        else if (copt.precision == Precision::Single)
             result.diagnostics.warnings.push_back("Precision::Single requested; propagated in double precision");
         result.diagnostics.hilbertSize = d;
         result.diagnostics.hierarchySize = impl.hierarchy_size();

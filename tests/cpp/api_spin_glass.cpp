@@ -2,7 +2,7 @@
 // (helix::HEOMSolver(options).run(system, hierarchy, solverOptions)) and
 // prints the result as JSON for tests/test_cpp_api.py to check against the
 // FP64 oracle.  Usage: api_spin_glass <spins> <seed> <h> <depth> <K> <steps> <dt> <mode>
-//   mode: final | trace | trajectory | legacy | sparse-bad
+//   mode: final | trace | trajectory | single | legacy | sparse-bad
 #include <helix/helix.h>
 
 #include <cstdio>
@@ -29,6 +29,7 @@ int main(int argc, char** argv)
     helix::SolverOptions solver;
     solver.steps = steps;
     solver.timeStep = dt;
+    if (mode == "single") options.precision = helix::Precision::Single;
     if (mode == "trace") solver.resultMode = helix::ResultMode::ObservableTrace;
     if (mode == "trajectory") solver.resultMode = helix::ResultMode::Trajectory;
     if (mode == "legacy") {
@@ -57,6 +58,7 @@ int main(int argc, char** argv)
     std::printf("], \"rho\": [");
     for (std::size_t i = 0; i < result.reduced_density.size(); ++i)
         std::printf("%s%.17g, %.17g", i ? ", " : "", result.reduced_density[i].real(), result.reduced_density[i].imag());
-    std::printf("], \"warnings\": %zu}\n", result.diagnostics.warnings.size());
+    std::printf("], \"warnings\": %zu, \"single\": %s}\n", result.diagnostics.warnings.size(),
+                result.diagnostics.precision == helix::Precision::Single ? "true" : "false");
     return 0;
 }

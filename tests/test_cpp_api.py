@@ -63,6 +63,28 @@ def test_cpp_api_matches_oracle(exe, mode):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("spins", [4, 7])
+def test_cpp_api_single_precision_request(exe, spins):
+    """Precision::Single runs the mixed path (complex64 hierarchy, FP64 tier-0
+    ADO) when 128 <= d <= 1024 and falls back to FP64 otherwise; either way
+    rho0 stays within trace distance 1e-6 of the FP64 oracle."""
+    seed, h, depth, K, steps, dt = 2031, 0.5, 2, 1, 20, 0.005
+    r = _run(exe, spins, seed, h, depth, K, steps, dt, "single")
+    assert r["ok"], r["codes"]
+    assert r["single"] is (spins == 7) and r["warnings"] >= 1
+    p = S.spin_glass(spins, seed=seed, depth=depth, K=K, h=h, dt=dt)
+    o = O.Oracle(p)
+    o.run(steps)
+    want = o.rho0()
+    o.close()
+    d = p.dim
+    rho = np.array(r["rho"]).view(np.complex128).reshape(d, d)
+    ev = np.linalg.eigvalsh(0.5 * ((rho - want) + (rho - want).conj().T))
+    tol = 1e-6 if spins == 7 else 1e-10
+    assert 0.5 * np.sum(np.abs(ev)) <= tol
+
+
+@pytest.mark.gpu
 def test_cpp_api_runs_the_reference_example(exe):
     """The reference's own example (examples/cpp/legacy_spin_glass.cpp): the
     compiled legacy system, compiled-default bath and hierarchy, 2 steps at the
