@@ -68,9 +68,9 @@ def load_peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def profiled_traffic(config: str) -> float | None:
-    """DRAM bytes per stage launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", f"fused_kernel_{config}_ncu.txt")
+def profiled_traffic(config: str, kernel: str = "fused_kernel") -> float | None:
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{config}_ncu.txt")
     try:
         with open(path) as f:
             for line in f:
@@ -270,7 +270,10 @@ def run_ours(args, cfg: dict) -> None:
     launch_ms = ms / (args.steps * stages)
     achieved = per_launch_bytes / (launch_ms / 1000.0) / 1e9
     peak, peak_kind = load_peaks()
-    traffic = profiled_traffic(args.config)
+    packed = bool(ctx.hermitian_packed)
+    kernel = "herm_kernel" if packed else "fused_kernel"
+    traffic = profiled_traffic(args.config, kernel)
+    slab_elems = p.dim * (p.dim + 1) // 2 if packed else p.dim * p.dim
 
     # ---- end to end through the C ABI with host buffers (e2e) --------------
     pinned = torch.empty(H * p.dim * p.dim * 2, dtype=torch.float64, pin_memory=True)
@@ -313,9 +316,11 @@ def run_ours(args, cfg: dict) -> None:
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
                          "algorithmic_bytes_per_launch": per_launch_bytes,
-                         "kernel": "fused_kernel<6,2> + upterm_kernel per stage", "launch_ms": launch_ms},
+                         "kernel": (f"{kernel}<{p.dim.bit_length() - 1}> + upterm_kernel per stage"
+                                    + (" (Hermitian-packed slabs)" if packed else "")),
+                         "launch_ms": launch_ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
-                    "d2h_bytes_per_step": p.dim * p.dim * 16 + 24,
+                    "d2h_bytes_per_step": slab_elems * 16 + 24,
                     "path": "hx_ctx_write_state (pinned host) + hx_ctx_step_trace (rho0, <H> per step) + hx_ctx_read_rho0"},
             "gpu_launches": launches,
             "clocks": clk,

@@ -25,6 +25,7 @@ STATUS_NAMES = {
 }
 PRECISION_DOUBLE = 1
 PRECISION_MIXED = 2  # complex64 hierarchy, ADO 0 (rho_0) in double precision
+FLAG_FULL_STATE = 1  # keep full d x d slabs on the device (d = 32, 64 default to Hermitian-packed)
 
 # Every exported symbol of include/helix_b200.h
 EXPORTS = [
@@ -201,7 +202,30 @@ def seeded_couplings(n: int, seed: int) -> np.ndarray:
     return J
 
 
-def _problem_struct(problem, order: int = 4, dt: float | None = None, precision: int = PRECISION_DOUBLE):
+def herm_index(r: int, c: int, d: int) -> int:
+    """Position of element (r, c), r <= c, in a Hermitian-packed slab of a
+    d x d matrix (the device layout of d = 32, 64 contexts): d/2 packed rows
+    of d + 1 elements, packed row s = row s from the diagonal on, then row
+    d-1-s from the diagonal on."""
+    return r * (d + 1) + (c - r) if r < d // 2 else (d - 1 - r) * (d + 1) + c + 1
+
+
+def unpack_herm(packed: np.ndarray, d: int) -> np.ndarray:
+    """Full d x d matrices from Hermitian-packed slabs (last axis d(d+1)/2)."""
+    packed = np.asarray(packed)
+    i = np.arange((d // 2) * (d + 1))
+    s, t = i // (d + 1), i % (d + 1)
+    first = t < d - s
+    r = np.where(first, s, d - 1 - s)
+    c = np.where(first, s + t, t - 1)
+    out = np.zeros(packed.shape[:-1] + (d, d), np.complex128)
+    out[..., c, r] = np.conj(packed)
+    out[..., r, c] = packed
+    return out
+
+
+def _problem_struct(problem, order: int = 4, dt: float | None = None, precision: int = PRECISION_DOUBLE,
+                    flags: int = 0):
     """hx_problem for a systems.Problem; returns (struct, keep-alive list)."""
     d = problem.dim
     n = problem.n_spins
@@ -228,7 +252,7 @@ def _problem_struct(problem, order: int = 4, dt: float | None = None, precision:
     keep.append(baths)
     prob = _Problem(d, hd.ctypes.data_as(C.POINTER(C.c_double)), hf.ctypes.data_as(C.POINTER(C.c_double)),
                     len(problem.baths), baths, problem.max_depth, problem.dt if dt is None else dt, order,
-                    precision, 0)
+                    precision, flags)
     return prob, keep
 
 
@@ -241,20 +265,28 @@ def rhs_noalloc(problem, rho_device_ptr: int, drho_device_ptr: int, stream_ptr: 
 
 
 class Context:
-    """One HEOM problem resident on the current CUDA device (wraps hx_ctx)."""
+    """One HEOM problem resident on the current CUDA device (wraps hx_ctx).
 
-    def __init__(self, problem, order: int = 4, dt: float | None = None, precision: str = "double"):
+    For d = 32, 64 the device keeps Hermitian-packed slabs and ``set_state``
+    accepts Hermitian ADOs only; ``full_state=True`` keeps full slabs for
+    general states (HX_FLAG_FULL_STATE)."""
+
+    def __init__(self, problem, order: int = 4, dt: float | None = None, precision: str = "double",
+                 full_state: bool = False):
         L = lib()
         self.problem = problem
         d = problem.dim
         prec = {"double": PRECISION_DOUBLE, "mixed": PRECISION_MIXED}[precision]
-        prob, self._keep = _problem_struct(problem, order, dt, prec)
+        prob, self._keep = _problem_struct(problem, order, dt, prec, FLAG_FULL_STATE if full_state else 0)
         h = C.c_void_p()
         _check(L.hx_ctx_create(C.byref(prob), C.byref(h)))
         self._h = h
         self.info = self.get_info()
         self.size = int(self.info.hierarchy_size)
         self.dim = d
+        # device slabs hold the upper triangle only (see herm_index)
+        self.hermitian_packed = (prec == PRECISION_DOUBLE and d >= 32 and
+                                 int(self.info.state_bytes) == self.size * (d * (d + 1) // 2) * 16)
 
     # lifecycle -----------------------------------------------------------
     def close(self) -> None:

@@ -519,16 +519,19 @@ __global__ void batch_gsum_kernel(const int32_t* rows, const int32_t* bath_off, 
 
 // trace[*counter % cap] = sum over instances of Tr(sigma_z(spin) rho_0); then ++*counter.
 // One block of 256 threads; fixed summation order, so the result does not depend on timing.
+// logd[i] carries bit 8 when instance i keeps Hermitian-packed slabs.
 __global__ void batch_obs_kernel(const double2* const* rho0, const int* logd, int count, int spin, double* trace,
                                  int* counter, int cap)
 {
     double s = 0.0;
     for (int i = threadIdx.x; i < count; i += blockDim.x) {
-        const int D = 1 << logd[i];
+        const int lg = logd[i] & 0xff;
+        const bool herm = (logd[i] >> 8) & 1;
+        const int D = 1 << lg;
         const double2* r0 = rho0[i];
         double v = 0.0;
         for (int r = 0; r < D; ++r) {
-            const double d = r0[static_cast<long long>(r) * D + r].x;
+            const double d = r0[herm ? herm_index(r, r, lg) : static_cast<long long>(r) * D + r].x;
             v += ((r >> spin) & 1) ? d : -d;
         }
         s += v;
@@ -842,7 +845,7 @@ void enqueue_batch_step(hx_batch* b, cudaStream_t s)
         launch_batch_stage(b, 0, 1, b->dt, hx::kBaseSelf, s);
         cudaMemcpyAsync(b->rho, b->ua, b->total_elems * sizeof(double2), cudaMemcpyDeviceToDevice, s);
         for (hx_ctx* c : b->ctxs)
-            cudaMemcpyAsync(c->rho, c->ua, static_cast<size_t>(c->H) * c->slab * sizeof(double2),
+            cudaMemcpyAsync(c->rho, c->ua, static_cast<size_t>(c->H) * c->slab_store * sizeof(double2),
                             cudaMemcpyDeviceToDevice, s);
     } else {
         int in = 0;
@@ -890,19 +893,21 @@ int build_context_launches(hx_batch* b)
     b->group_of.assign(nc, 0);
     std::vector<int> order(nc);
     for (int k = 0; k < nc; ++k) order[k] = k;
-    std::sort(order.begin(), order.end(), [&](int x, int y) { return b->ctxs[x]->H * b->ctxs[x]->slab > b->ctxs[y]->H * b->ctxs[y]->slab; });
+    std::sort(order.begin(), order.end(), [&](int x, int y) {
+        return b->ctxs[x]->H * b->ctxs[x]->slab_store > b->ctxs[y]->H * b->ctxs[y]->slab_store;
+    });
     std::vector<long long> load(std::max(1, b->ngroups), 0);
     for (int k : order) {
         const int g = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
         b->group_of[k] = g;
-        load[g] += b->ctxs[k]->H * static_cast<long long>(b->ctxs[k]->slab);
+        load[g] += b->ctxs[k]->H * static_cast<long long>(b->ctxs[k]->slab_store);
     }
     b->fargs.resize(nc);
     for (int k = 0; k < nc; ++k) {
         b->fargs[k] = hx::fused_args_of(b->ctxs[k]);
         b->fargs[k].error_flag = b->error_flag;
         // the kernel's shared-memory limit is raised here, outside any stream capture
-        if (!hx::prepare_fused(b->ctxs[k]->logd, b->ctxs[k]->M, b->ctxs[k]->J))
+        if (!hx::prepare_fused(b->ctxs[k]->logd, b->ctxs[k]->M, b->ctxs[k]->J, b->ctxs[k]->herm ? 1 : 0))
             return fail(HX_ERR_UNSUPPORTED_EXECUTION, "fused kernel tables exceed shared memory");
     }
     for (int g = 1; g < b->ngroups; ++g) {
@@ -919,7 +924,7 @@ int build_context_launches(hx_batch* b)
     for (int i = 0; i < b->count; ++i) {
         const int k = b->large_of[i];
         rp[i] = k >= 0 ? b->ctxs[k]->rho : b->rho + b->h_inst[i].state_off;
-        lgs[i] = b->h_inst[i].logd;
+        lgs[i] = b->h_inst[i].logd | ((k >= 0 && b->ctxs[k]->herm) ? 1 << 8 : 0);
     }
     int rc = HX_OK;
     if ((rc = balloc(b, &b->rho0_ptr, b->count)) || (rc = balloc(b, &b->logd_arr, b->count))) return rc;
@@ -930,16 +935,6 @@ int build_context_launches(hx_batch* b)
     return HX_OK;
 }
 
-// Spin p with coupling_diag[r] = +1 where bit p of r is set and -1 elsewhere, or -1.
-int pauli_spin(const double* v, int D)
-{
-    for (int p = 0; (1 << p) < D; ++p) {
-        bool ok = true;
-        for (int r = 0; r < D && ok; ++r) ok = v[r] == (((r >> p) & 1) ? 1.0 : -1.0);
-        if (ok) return p;
-    }
-    return -1;
-}
 
 }  // namespace
 
@@ -965,7 +960,7 @@ int hx_batch_create(const hx_problem* problems, uint32_t count, const hx_batch_o
         if (order < 1 || order > 8) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "integration_order must be in 1..8");
         if (p.n_baths == 0 || !p.baths || p.n_baths > 16) return fail(HX_ERR_UNSUPPORTED_BATH, "batched instances need 1..16 baths");
         if (p.max_depth < 1) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "max_depth must be >= 1");
-        if (p.flags != 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "flags must be 0");
+        if ((p.flags & ~HX_FLAG_FULL_STATE) != 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "unknown flags");
         for (uint32_t j = 0; j < p.n_baths; ++j) {
             const hx_bath& bb = p.baths[j];
             if (!bb.coupling_diag) return fail(HX_ERR_UNSUPPORTED_BATH, "bath coupling operator is NULL");
@@ -973,7 +968,7 @@ int hx_batch_create(const hx_problem* problems, uint32_t count, const hx_batch_o
                 for (uint32_t k = 0; (1u << k) < d; ++k)
                     if (bb.coupling_flip[k] != 0.0)
                         return fail(HX_ERR_UNSUPPORTED_EXECUTION, "batched instances need sigma_z couplings");
-            if (pauli_spin(bb.coupling_diag, static_cast<int>(d)) < 0)
+            if (hx::pauli_spin(bb.coupling_diag, static_cast<int>(d)) < 0)
                 return fail(HX_ERR_UNSUPPORTED_EXECUTION, "batched instances need sigma_z couplings (+-1 by one spin bit)");
         }
     }
@@ -1103,7 +1098,7 @@ int hx_batch_create(const hx_problem* problems, uint32_t count, const hx_batch_o
         blk.insert(blk.end(), nu.begin(), nu.end());
         blk.insert(blk.end(), tc.begin(), tc.end());
         for (int j = 0; j < J; ++j) blk.push_back(bc[j].theta_a);
-        for (int j = 0; j < J; ++j) blk.push_back(pauli_spin(p.baths[j].coupling_diag, D));
+        for (int j = 0; j < J; ++j) blk.push_back(hx::pauli_spin(p.baths[j].coupling_diag, D));
         for (int j = 0; j < J; ++j) blk.push_back(bc[j].offset);
         blk.push_back(M);
         if (blk.size() & 1) blk.push_back(0.0);  // 16-byte aligned blocks
@@ -1243,7 +1238,7 @@ int hx_batch_info(const hx_batch* b, hx_batch_stats* info)
     info->count = static_cast<uint32_t>(b->count);
     info->total_ados = static_cast<uint64_t>(b->total_ados);
     uint64_t ctx_bytes = 0;
-    for (const hx_ctx* c : b->ctxs) ctx_bytes += static_cast<uint64_t>(c->H) * c->slab * sizeof(double2);
+    for (const hx_ctx* c : b->ctxs) ctx_bytes += static_cast<uint64_t>(c->H) * c->slab_store * sizeof(double2);
     info->state_bytes = static_cast<uint64_t>(b->total_elems) * sizeof(double2) + ctx_bytes;
     info->device_bytes = b->device_bytes;
     for (const hx_ctx* c : b->ctxs) info->device_bytes += c->device_bytes;
@@ -1351,6 +1346,13 @@ int hx_batch_read_rho0(hx_batch* b, uint32_t instance, double* out, uint64_t n)
     if (n < 2 * d2) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "output buffer too small");
     const int k = b->large_of[instance];
     const double2* src = k >= 0 ? b->ctxs[k]->rho : b->rho + in.state_off;
+    if (k >= 0 && b->ctxs[k]->herm) {
+        std::vector<double2> pk(b->ctxs[k]->slab_store);
+        HX_CUDA_TRY(cudaMemcpyAsync(pk.data(), src, pk.size() * sizeof(double2), cudaMemcpyDeviceToHost, b->stream));
+        HX_CUDA_TRY(cudaStreamSynchronize(b->stream));
+        hx::unpack_herm_host(pk.data(), in.logd, out);
+        return batch_check_flag(b);
+    }
     HX_CUDA_TRY(cudaMemcpyAsync(out, src, d2 * sizeof(double2), cudaMemcpyDeviceToHost, b->stream));
     HX_CUDA_TRY(cudaStreamSynchronize(b->stream));
     return batch_check_flag(b);

@@ -53,7 +53,7 @@ void release(hx_ctx* c)
                     c->trace_buf, c->energy_buf, c->diag_table, c->ent_count, c->ent_slab, c->ent_bath,
                     c->ent_wc, c->ent_wa, c->order_perm, c->ado_keep, c->up_slot, c->up_ado, c->up_cnt,
                     c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf, c->rho32, c->ua32, c->ub32,
-                    c->U32, c->diag32, c->vdiag32, c->hflip32};
+                    c->U32, c->diag32, c->vdiag32, c->hflip32, c->diag_herm, c->vbit};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -88,7 +88,7 @@ hx::StageTables tables_of(const hx_ctx* c)
 hx::FusedArgs hx::fused_args_of(const hx_ctx* c)
 {
     hx::FusedArgs a{};
-    a.diag = c->diag_table;
+    a.diag = c->herm ? c->diag_herm : c->diag_table;
     a.vdiag = c->vdiag;
     a.hflip = c->hflip;
     a.gsum = c->gsum;
@@ -106,12 +106,30 @@ hx::FusedArgs hx::fused_args_of(const hx_ctx* c)
     a.M = c->M;
     a.J = c->J;
     a.logd = c->logd;
+    a.herm = c->herm ? 1 : 0;
+    a.vbit = c->vbit;
+    a.pauli = c->vbit ? 1 : 0;
     return a;
 }
 
 hx::UpTermArgs hx::upterm_args_of(const hx_ctx* c)
 {
-    return hx::UpTermArgs{c->vdiag, c->up_cnt, c->up_slab, c->up_bath, c->bath_off, c->up_slots, c->M, c->J, c->logd};
+    return hx::UpTermArgs{c->vdiag, c->up_cnt, c->up_slab, c->up_bath, c->bath_off, c->up_slots,
+                          c->M,     c->J,      c->logd,    c->herm ? 1 : 0};
+}
+
+void hx::unpack_herm_host(const double2* pk, int logd, double* out)
+{
+    const int D = 1 << logd, P = hx::herm_elems(logd);
+    for (int i = 0; i < P; ++i) {
+        int r, c;
+        hx::herm_coords(i, logd, r, c);
+        const double2 v = pk[i];
+        out[2 * (static_cast<size_t>(r) * D + c)] = v.x;
+        out[2 * (static_cast<size_t>(r) * D + c) + 1] = v.y;
+        out[2 * (static_cast<size_t>(c) * D + r)] = v.x;
+        out[2 * (static_cast<size_t>(c) * D + r) + 1] = r == c ? v.y : -v.y;
+    }
 }
 
 namespace {
@@ -306,6 +324,36 @@ int read_error_flag(hx_ctx* c)
     return HX_OK;
 }
 
+// Packed slab from a full row-major complex matrix (2 d^2 doubles); false
+// when the matrix is not Hermitian to 1e-12 of its largest element.
+bool pack_herm_host(const double* in, int logd, double2* pk)
+{
+    const int D = 1 << logd, P = hx::herm_elems(logd);
+    double scale = 0.0;
+    for (size_t e = 0; e < static_cast<size_t>(D) * D; ++e) scale = std::max(scale, std::hypot(in[2 * e], in[2 * e + 1]));
+    const double tol = 1e-12 * scale;
+    for (int i = 0; i < P; ++i) {
+        int r, c;
+        hx::herm_coords(i, logd, r, c);
+        const size_t up = static_cast<size_t>(r) * D + c, lo = static_cast<size_t>(c) * D + r;
+        if (r != c && std::hypot(in[2 * up] - in[2 * lo], in[2 * up + 1] + in[2 * lo + 1]) > tol) return false;
+        pk[i] = make_double2(in[2 * up], in[2 * up + 1]);
+    }
+    return true;
+}
+
+// count slabs of a packed device buffer into full matrices on the host.
+int read_herm(hx_ctx* c, const double2* src, size_t count, double* out)
+{
+    std::vector<double2> tmp(count * c->slab_store);
+    HX_CUDA_TRY(cudaMemcpyAsync(tmp.data(), src, tmp.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->counters.d2h_bytes += tmp.size() * sizeof(double2);
+    for (size_t k = 0; k < count; ++k)
+        hx::unpack_herm_host(tmp.data() + k * c->slab_store, c->logd, out + 2 * k * c->slab);
+    return HX_OK;
+}
+
 // Mixed precision: the whole state as complex128 on the host (complex64
 // hierarchy widened, ADO 0 from its double-precision slab); src32/src64 are
 // matching buffers (rho32/rho, ua32/ua, ...).
@@ -393,7 +441,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     if (p->n_baths == 0 || !p->baths) return fail(HX_ERR_UNSUPPORTED_BATH, "at least one bath is required");
     if (p->n_baths > static_cast<uint32_t>(hx::kMaxBaths)) return fail(HX_ERR_UNSUPPORTED_BATH, "too many baths");
     if (p->max_depth < 1) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "max_depth must be >= 1");
-    if (p->flags != 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "flags must be 0");
+    if ((p->flags & ~HX_FLAG_FULL_STATE) != 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "unknown flags");
 
     const int J = static_cast<int>(p->n_baths);
     std::vector<hx::BathConst> bc(J);
@@ -436,7 +484,6 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     if (e != cudaSuccess) return bail(hx::cuda_fail(e, "cudaStreamCreate"));
     c->stream = c->own_stream;
 
-    const size_t nstate = static_cast<size_t>(H) * c->slab;
     // spin-flip parts in any coupling operator select the two-pass flip path
     std::vector<double> vf(static_cast<size_t>(J) * logd, 0.0);
     bool any_flip = false;
@@ -453,6 +500,15 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     c->mixed = p->precision == HX_PRECISION_MIXED;
     if (c->mixed && !c->use_large)
         return bail(fail(HX_ERR_UNSUPPORTED_PRECISION, "mixed precision needs diagonal coupling operators"));
+    // fused stage kernels (d = 32, 64), on Hermitian-packed slabs unless the caller keeps full slabs
+    const char* force_generic = std::getenv("HX_FORCE_GENERIC_STAGE");
+    const bool want_herm = (p->flags & HX_FLAG_FULL_STATE) == 0;
+    const bool fused_ok = !c->use_flip && !c->use_large && logd >= 5 && logd <= hx::kMaxLogD &&
+                          hx::fused_supported(logd, M, J, want_herm ? 1 : 0) &&
+                          !(force_generic && force_generic[0] == '1');
+    c->herm = fused_ok && want_herm;
+    c->slab_store = c->herm ? static_cast<size_t>(hx::herm_elems(logd)) : c->slab;
+    const size_t nstate = static_cast<size_t>(H) * c->slab_store;
     if ((rc = dev_alloc(c, &c->vflip, vf.size())) || (rc = upload(c, c->vflip, vf))) return bail(rc);
     if (c->use_flip && (rc = dev_alloc(c, &c->Bbuf, nstate * J))) return bail(rc);
     // double-precision state: the whole hierarchy, or only ADO 0 in mixed precision
@@ -523,7 +579,8 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     if (rc == HX_OK) {
         hx::launch_coefficients(c->rows, c->H, M, J, dmb, dmk, dnu, dtc, dta, dphi, c->bath_off, c->acoef,
                                 c->bcoef, c->gsum, c->stream);
-        hx::launch_init_state(c->rho, static_cast<long long>(n64), c->d, c->stream);
+        const long long one = c->herm ? hx::herm_index(c->d - 1, c->d - 1, logd) : static_cast<long long>(c->slab) - 1;
+        hx::launch_init_state(c->rho, static_cast<long long>(n64), one, c->stream);
         if (c->mixed) {
             e = cudaMemsetAsync(c->rho32, 0, nstate * sizeof(float2), c->stream);
             if (e == cudaSuccess) hx::launch_d2f(c->rho, c->rho32, static_cast<long long>(c->slab), c->stream);
@@ -532,9 +589,6 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
         rc = check_launch("setup kernels");
     }
     // fused stage kernel (d = 32, 64): neighbour entry lists, diagonal table, up-term tables
-    const char* force_generic = std::getenv("HX_FORCE_GENERIC_STAGE");
-    const bool fused_ok = !c->use_flip && !c->use_large && logd >= 5 && logd <= hx::kMaxLogD &&
-                          hx::fused_supported(logd, M, J) && !(force_generic && force_generic[0] == '1');
     if (rc == HX_OK && (fused_ok || c->use_large)) {
         cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
         int* dS = nullptr;
@@ -545,6 +599,13 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
             (rc = dev_alloc(c, &c->up_ado, H)) || (rc = dev_alloc(c, &c->up_cnt, H)) || (rc = dev_alloc(c, &dS, 1))) {
         } else {
             hx::launch_diag_table(c->hdiag, c->vdiag, c->xi, c->counter, c->d, J, c->diag_table, c->stream);
+            if (c->herm && (rc = dev_alloc(c, &c->diag_herm, c->slab_store)) == HX_OK)
+                hx::launch_pack_herm(c->diag_table, logd, c->diag_herm, c->stream);
+            // sigma_z couplings: the fused kernels take v_r from bit r of the spin, not from a table
+            std::vector<int> bits(J);
+            bool all_pauli = true;
+            for (int j = 0; j < J; ++j) all_pauli = all_pauli && (bits[j] = hx::pauli_spin(vd.data() + static_cast<size_t>(j) * d, c->d)) >= 0;
+            if (rc == HX_OK && all_pauli && (rc = dev_alloc(c, &c->vbit, J)) == HX_OK) rc = upload(c, c->vbit, bits);
             hx::launch_entries(c->rows, c->edges, c->acoef, c->bcoef, c->bath_off, c->H, M, J,
                                static_cast<int>(p->max_depth), c->ent_count, c->ent_slab, c->ent_bath, c->ent_wc,
                                c->ent_wa, c->ado_keep, c->stream);
@@ -566,7 +627,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                     if (rc == HX_OK) rc = dev_alloc(c, &c->up_bath, static_cast<size_t>(S) * M);
                     if (rc == HX_OK) {
                         if (c->mixed) rc = dev_alloc(c, &c->U32, static_cast<size_t>(S) * c->slab);
-                        else rc = dev_alloc(c, &c->U, static_cast<size_t>(S) * c->slab);
+                        else rc = dev_alloc(c, &c->U, static_cast<size_t>(S) * c->slab_store);
                     }
                     if (rc == HX_OK) {
                         e = cudaMemcpyAsync(c->up_slab, tmp_slab, static_cast<size_t>(S) * M * sizeof(int32_t),
@@ -646,7 +707,7 @@ int hx_ctx_info(const hx_ctx* c, hx_info* info)
     info->dim = static_cast<uint32_t>(c->d);
     info->modes = static_cast<uint32_t>(c->M);
     info->hierarchy_size = static_cast<uint64_t>(c->H);
-    info->state_bytes = static_cast<uint64_t>(c->H) * c->slab * sizeof(double2);
+    info->state_bytes = static_cast<uint64_t>(c->H) * c->slab_store * sizeof(double2);
     info->device_bytes = c->device_bytes;
     info->steps_done = c->steps_done;
     info->time = static_cast<double>(c->steps_done) * c->dt;
@@ -704,18 +765,19 @@ int hx_ctx_step_trace(hx_ctx* c, uint64_t nsteps, double* rho0_trace, double* en
         const int chunk = static_cast<int>(std::min<uint64_t>(nsteps - done, c->trace_cap));
         for (int t = 0; t < chunk; ++t) {
             enqueue_step(c);
-            hx::launch_observables(c->rho, c->logd, c->hdiag, c->hflip, nullptr, c->energy_buf + 3 * t, c->stream);
+            hx::launch_observables(c->rho, c->logd, c->herm, c->hdiag, c->hflip, nullptr, c->energy_buf + 3 * t,
+                                   c->stream);
             c->counters.kernel_launches += 1;
             if (rho0_trace)
-                HX_CUDA_TRY(cudaMemcpyAsync(c->trace_buf + static_cast<size_t>(t) * c->slab, c->rho,
-                                            c->slab * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+                HX_CUDA_TRY(cudaMemcpyAsync(c->trace_buf + static_cast<size_t>(t) * c->slab_store, c->rho,
+                                            c->slab_store * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
         }
         int rc = check_launch("trace step");
         if (rc != HX_OK) return rc;
         if (rho0_trace) {
-            HX_CUDA_TRY(cudaMemcpyAsync(pin_rho, c->trace_buf, chunk * c->slab * sizeof(double2),
+            HX_CUDA_TRY(cudaMemcpyAsync(pin_rho, c->trace_buf, chunk * c->slab_store * sizeof(double2),
                                         cudaMemcpyDeviceToHost, c->stream));
-            c->counters.d2h_bytes += chunk * c->slab * sizeof(double2);
+            c->counters.d2h_bytes += chunk * c->slab_store * sizeof(double2);
         }
         if (energy_trace) {
             HX_CUDA_TRY(cudaMemcpyAsync(pin_en, c->energy_buf, chunk * 3 * sizeof(double), cudaMemcpyDeviceToHost,
@@ -723,8 +785,13 @@ int hx_ctx_step_trace(hx_ctx* c, uint64_t nsteps, double* rho0_trace, double* en
             c->counters.d2h_bytes += chunk * 3 * sizeof(double);
         }
         HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        if (rho0_trace)
+        if (rho0_trace && c->herm) {
+            for (int t = 0; t < chunk; ++t)
+                hx::unpack_herm_host(reinterpret_cast<const double2*>(pin_rho) + static_cast<size_t>(t) * c->slab_store,
+                                     c->logd, rho0_trace + (done + t) * c->slab * 2);
+        } else if (rho0_trace) {
             std::memcpy(rho0_trace + done * c->slab * 2, pin_rho, chunk * c->slab * sizeof(double2));
+        }
         if (energy_trace)
             for (int t = 0; t < chunk; ++t) energy_trace[done + t] = pin_en[3 * t];
         done += chunk;
@@ -736,6 +803,10 @@ int hx_ctx_read_rho0(hx_ctx* c, double* out, uint64_t n)
 {
     if (!c || !out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
     if (n < 2 * c->slab) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "output buffer too small");
+    if (c->herm) {
+        const int rc = read_herm(c, c->rho, 1, out);
+        return rc != HX_OK ? rc : read_error_flag(c);
+    }
     HX_CUDA_TRY(cudaMemcpyAsync(out, c->rho, c->slab * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->counters.d2h_bytes += c->slab * sizeof(double2);
@@ -745,7 +816,7 @@ int hx_ctx_read_rho0(hx_ctx* c, double* out, uint64_t n)
 int hx_ctx_observables(hx_ctx* c, double* energy, double* trace_re, double* trace_im)
 {
     if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
-    hx::launch_observables(c->rho, c->logd, c->hdiag, c->hflip, nullptr, c->obs, c->stream);
+    hx::launch_observables(c->rho, c->logd, c->herm, c->hdiag, c->hflip, nullptr, c->obs, c->stream);
     c->counters.kernel_launches += 1;
     int rc = check_launch("observables kernel");
     if (rc != HX_OK) return rc;
@@ -767,6 +838,10 @@ int hx_ctx_read_state(hx_ctx* c, double* out, uint64_t n)
         const int rc = read_mixed(c, c->rho32, c->rho, out);
         return rc != HX_OK ? rc : read_error_flag(c);
     }
+    if (c->herm) {
+        const int rc = read_herm(c, c->rho, static_cast<size_t>(c->H), out);
+        return rc != HX_OK ? rc : read_error_flag(c);
+    }
     HX_CUDA_TRY(cudaMemcpyAsync(out, c->rho, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->counters.d2h_bytes += count * sizeof(double2);
@@ -785,6 +860,19 @@ int hx_ctx_write_state(hx_ctx* c, const double* in, uint64_t n)
         HX_CUDA_TRY(cudaMemcpyAsync(c->rho32, tmp.data(), count * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
         HX_CUDA_TRY(cudaMemcpyAsync(c->rho, in, c->slab * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
         c->counters.h2d_bytes += count * sizeof(float2) + c->slab * sizeof(double2);
+        HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return HX_OK;
+    }
+    if (c->herm) {
+        std::vector<double2> pk(static_cast<size_t>(c->H) * c->slab_store);
+        for (long long k = 0; k < c->H; ++k)
+            if (!pack_herm_host(in + 2 * static_cast<size_t>(k) * c->slab, c->logd, pk.data() + k * c->slab_store))
+                return fail(HX_ERR_INVALID_RUNTIME_OPTION,
+                            "ADO " + std::to_string(k) +
+                                " is not Hermitian; this context keeps Hermitian-packed slabs (create it with "
+                                "HX_FLAG_FULL_STATE for general states)");
+        HX_CUDA_TRY(cudaMemcpyAsync(c->rho, pk.data(), pk.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        c->counters.h2d_bytes += pk.size() * sizeof(double2);
         HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
         return HX_OK;
     }
@@ -811,6 +899,10 @@ int hx_ctx_rhs(hx_ctx* c, double* out, uint64_t n)
     if (rc != HX_OK) return rc;
     if (c->mixed) {
         rc = read_mixed(c, c->ua32, c->ua, out);
+        return rc != HX_OK ? rc : read_error_flag(c);
+    }
+    if (c->herm) {
+        rc = read_herm(c, c->ua, static_cast<size_t>(c->H), out);
         return rc != HX_OK ? rc : read_error_flag(c);
     }
     HX_CUDA_TRY(cudaMemcpyAsync(out, c->ua, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
@@ -847,7 +939,7 @@ int hx_ctx_check_finite(hx_ctx* c)
     int host = 0;
     int* scratch = reinterpret_cast<int*>(c->obs + 3);
     HX_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(int), c->stream));
-    hx::launch_finite_check(c->rho, static_cast<long long>(c->H) * c->slab, scratch, c->stream);
+    hx::launch_finite_check(c->rho, static_cast<long long>(c->H) * c->slab_store, scratch, c->stream);
     c->counters.kernel_launches += 1;
     int rc = check_launch("finite check");
     if (rc != HX_OK) return rc;

@@ -1,4 +1,5 @@
-// Multi-CTA fused stage kernel for d = 32 and d = 64 (FP64).
+// Multi-CTA fused stage kernels for d = 32 and d = 64 (FP64), on full or on
+// Hermitian-packed slabs.
 //
 // Same mathematics as stage_kernel (hx_stage.cu): one launch evaluates
 // out_n = base_n + alpha L(u)_n for every ADO n, L being the reference
@@ -84,6 +85,12 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
             "r"(s_addr(dst)),
         "l"(src), "r"(bytes), "r"(s_addr(bar)), "l"(pol)
         : "memory");
+}
+
+// Start pulling `bytes` at src into L2 (no completion to wait for).
+__device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
 // Bounded wait on an mbarrier phase; false if the poll budget ran out.
@@ -280,6 +287,272 @@ __global__ void __launch_bounds__(256, MINB)
     fused_ado<LOGD>(a, n, u, rho, out, alpha, base_kind);
 }
 
+// ---------------------------------------------------------------------------
+// Hermitian-packed variant.  Slabs, the Horner base, neighbours, up terms,
+// the diagonal table and the output are packed upper triangles (herm_index
+// in hx_internal.h), so every stream moves d(d+1)/2 elements instead of d^2.
+// Thread t owns packed elements t + T k; a warp's 32 elements are
+// consecutive in the packed slab, so neighbour, up-term, base and output
+// accesses coalesce, and they are runs of consecutive columns of at most two
+// matrix rows.
+//
+// The CTA unpacks its own slab into a full d x d copy in shared memory for
+// the transverse-field flips, element (r, c) in slot r d + (c ^ (r & 7)).
+// With that swizzle every flip is one XOR of the slot with a constant
+// (row bit b: d 2^b, plus 2^b when b < 3; column bit b: 2^b), and the
+// accesses stay free of bank conflicts: a run of consecutive columns of one
+// row, its row flips and its column flips each cover eight distinct
+// 16-byte bank groups per quarter-warp, and so do the mirrored writes (c, r)
+// of the unpack, one column of consecutive rows.  With PAULI every coupling
+// operator is sigma_z of one spin: v_r = +1 or -1 from a bit of r, and of
+// [V, X] and {V, X} exactly one is nonzero at each element.
+template <int LOGD> struct HermShape;
+template <> struct HermShape<5> { static constexpr int T = 192, MINB = 4; };  // 528 elements: 3 per thread
+template <> struct HermShape<6> { static constexpr int T = 416, MINB = 2; };  // 2080 elements: 5 per thread
+
+constexpr unsigned kPrefetchAhead = 148;  // CTAs per resident wave per unit of HermShape::MINB
+
+template <int LOGD>
+__device__ __forceinline__ int herm_slot(int r, int c)
+{
+    return (r << LOGD) | (c ^ (r & 7));
+}
+
+template <int LOGD, bool PAULI>
+__device__ __forceinline__ void herm_ado(const FusedArgs& a, long long n, const double2* __restrict__ u,
+                                         const double2* rho, double2* out, double alpha, int base_kind)
+{
+    constexpr int D = 1 << LOGD, HALF = D / 2, P = HALF * (D + 1);
+    constexpr int T = HermShape<LOGD>::T, E = (P + T - 1) / T;
+    constexpr bool kExact = (P % T) == 0;
+    extern __shared__ __align__(128) unsigned char smem[];
+    double2* full = reinterpret_cast<double2*>(smem);  // [D * D] own slab, unpacked and swizzled
+    double2* pk = full + D * D;                         // [P] own packed slab, then the packed rho slab
+    uint64_t* bar = reinterpret_cast<uint64_t*>(pk + P);
+    double* sV = reinterpret_cast<double*>(bar + 2);   // [J][D] (general couplings)
+    double* sH = sV + a.J * D;                          // [LOGD]
+    double* sWc = sH + LOGD;                            // [2M]
+    double* sWa = sWc + 2 * a.M;                        // [2M]
+    int* sSlab = reinterpret_cast<int*>(sWa + 2 * a.M);
+    int* sBath = sSlab + 2 * a.M;
+    int* sBit = sBath + 2 * a.M;                        // [J] (PAULI)
+
+    const int tid = threadIdx.x;
+    const uint64_t pkeep = pol_last(), pn = pol_normal();
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(&bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(&bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) bulk_g2s(pk, u + n * P, P * sizeof(double2), &bar[0], a.ado_keep[n] ? pkeep : pn);
+    const int Q = a.ent_count[n];
+    if (PAULI) {
+        if (tid < a.J) sBit[tid] = a.vbit[tid];
+    } else {
+        for (int i = tid; i < a.J * D; i += T) sV[i] = a.vdiag[i];
+    }
+    if (tid < LOGD) sH[tid] = a.hflip[tid];
+    for (int q = tid; q < Q; q += T) {
+        const long long src = n * 2 * a.M + q;
+        sSlab[q] = a.ent_slab[src];
+        sBath[q] = a.ent_bath[src];
+        sWc[q] = a.ent_wc[src];
+        sWa[q] = a.ent_wa[src];
+    }
+    const double g = a.gsum[n];
+    const int slot = a.slot ? a.slot[n] : -1;
+    __syncthreads();
+    if (__syncthreads_or(!bar_wait(&bar[0], 0))) {
+        if (tid == 0) atomicExch(a.error_flag, 1);
+        return;
+    }
+
+    // ---- unpack the own slab: (r, c) and its mirror (c, r) = conj
+    int rc[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        const int i = tid + T * k;
+        int r = 0, c = 0;
+        if (kExact || i < P) {
+            herm_coords(i, LOGD, r, c);
+            const double2 v = pk[i];
+            full[herm_slot<LOGD>(r, c)] = v;
+            if (r != c) full[herm_slot<LOGD>(c, r)] = make_double2(v.x, -v.y);
+        }
+        rc[k] = (r << 8) | c;
+    }
+    __syncthreads();
+    // the packed copy is still the stage-1 base; otherwise stream rho_n into it
+    if (base_kind == kBaseRho && tid == 0) bulk_g2s(pk, rho + n * P, P * sizeof(double2), &bar[1], pol_first());
+
+    // ---- step A: diagonal (packed table) and transverse field (unpacked slab)
+    double2 acc[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        const int i = tid + T * k;
+        acc[k] = make_double2(0.0, 0.0);
+        if (!kExact && i >= P) continue;
+        const int sl = herm_slot<LOGD>(rc[k] >> 8, rc[k] & 255);
+        const double2 x = full[sl];
+        const double2 t = __ldg(a.diag + i);
+        double hr = 0.0, hi = 0.0;
+#pragma unroll
+        for (int b = 0; b < LOGD; ++b) {
+            const double h = sH[b];
+            const double2 rowp = full[sl ^ ((1 << b) << LOGD) ^ (b < 3 ? (1 << b) : 0)];
+            const double2 colp = full[sl ^ (1 << b)];
+            hr += h * (rowp.x - colp.x);
+            hi += h * (rowp.y - colp.y);
+        }
+        const double tr = t.x - g;
+        acc[k].x = tr * x.x - t.y * x.y + hi;
+        acc[k].y = tr * x.y + t.y * x.x - hr;
+    }
+
+    // ---- step B: neighbour entries, E loads in flight per thread
+    const double2* ubase = u + tid;
+    for (int q = 0; q < Q; ++q) {
+        const int jb = sBath[q];
+        const int j = jb & 0xffff;
+        const uint64_t pol = (jb >> 16) ? pkeep : pn;
+        const double wc = sWc[q], wa = sWa[q];
+        const double2* src = ubase + static_cast<long long>(sSlab[q]) * P;
+        double2 y[E];
+        if (PAULI) {
+            // v = +-1 from bit `bit`: equal bits of r and c -> only {V, X} = +-2 X;
+            // different bits -> only [V, X] = +-2 X (sign + when bit r is set)
+            const int bit = sBit[j];
+            const bool need_same = wa != 0.0, need_diff = wc != 0.0;
+#pragma unroll
+            for (int k = 0; k < E; ++k) {
+                const int br = (rc[k] >> (8 + bit)) & 1, bc = (rc[k] >> bit) & 1;
+                y[k] = make_double2(0.0, 0.0);
+                if ((kExact || tid + T * k < P) && (br == bc ? need_same : need_diff))
+                    y[k] = ldg_hint(src + T * k, pol);
+            }
+            const double a2 = 2.0 * wa, c2 = 2.0 * wc;
+#pragma unroll
+            for (int k = 0; k < E; ++k) {
+                const int br = (rc[k] >> (8 + bit)) & 1, bc = (rc[k] >> bit) & 1;
+                const bool same = br == bc;
+                // -(vr + vc) wa {V,.} term (real weight) or -i (vr - vc) wc [V,.] term
+                const double w = same ? (br ? -a2 : a2) : (br ? -c2 : c2);
+                const double px = same ? y[k].x : -y[k].y;
+                const double py = same ? y[k].y : y[k].x;
+                acc[k].x += w * px;
+                acc[k].y += w * py;
+            }
+        } else {
+            const double* vj = sV + j * D;
+#pragma unroll
+            for (int k = 0; k < E; ++k) {
+                const double vr = vj[rc[k] >> 8], vc = vj[rc[k] & 255];
+                y[k] = make_double2(0.0, 0.0);
+                if ((kExact || tid + T * k < P) && ((vr + vc) * wa != 0.0 || (vr - vc) * wc != 0.0))
+                    y[k] = ldg_hint(src + T * k, pol);
+            }
+#pragma unroll
+            for (int k = 0; k < E; ++k) {
+                const double vr = vj[rc[k] >> 8], vc = vj[rc[k] & 255];
+                const double ar = -(vr + vc) * wa, ai = -(vr - vc) * wc;
+                acc[k].x += ar * y[k].x - ai * y[k].y;
+                acc[k].y += ar * y[k].y + ai * y[k].x;
+            }
+        }
+    }
+    // ---- up term of tier L-1, summed by upterm_kernel
+    if (slot >= 0) {
+        const double2* Un = a.U + static_cast<long long>(slot) * P + tid;
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+            if (!kExact && tid + T * k >= P) continue;
+            const double2 w = ldg_stream(Un + T * k);
+            acc[k].x += w.x;
+            acc[k].y += w.y;
+        }
+    }
+
+    // ---- Horner epilogue
+    if (base_kind == kBaseRho && __syncthreads_or(!bar_wait(&bar[1], 0))) {
+        if (tid == 0) atomicExch(a.error_flag, 1);
+        return;
+    }
+    double2* out_n = out + n * P + tid;
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        if (!kExact && tid + T * k >= P) continue;
+        const double2 b = (base_kind == kBaseZero) ? make_double2(0.0, 0.0) : pk[tid + T * k];
+        stg_stream(out_n + T * k, make_double2(b.x + alpha * acc[k].x, b.y + alpha * acc[k].y));
+    }
+}
+
+template <int LOGD, bool PAULI>
+__global__ void __launch_bounds__(HermShape<LOGD>::T, HermShape<LOGD>::MINB)
+    herm_kernel(FusedArgs a, const double2* __restrict__ u, const double2* rho, double2* out, double alpha,
+                int base_kind)
+{
+    const long long n = a.order ? static_cast<long long>(a.order[blockIdx.x]) : static_cast<long long>(blockIdx.x);
+    // The CTA that starts one resident wave later (MINB CTAs on each of 148
+    // SMs) finds its slab and its Horner base in L2 instead of waiting on DRAM.
+    constexpr unsigned ahead = kPrefetchAhead * HermShape<LOGD>::MINB;
+    if (threadIdx.x == 0 && blockIdx.x + ahead < gridDim.x) {
+        constexpr uint32_t bytes = (1u << (LOGD - 1)) * ((1u << LOGD) + 1) * sizeof(double2);
+        const long long m = a.order ? a.order[blockIdx.x + ahead] : blockIdx.x + ahead;
+        prefetch_l2(u + m * (bytes / sizeof(double2)), bytes);
+        if (base_kind == kBaseRho) prefetch_l2(rho + m * (bytes / sizeof(double2)), bytes);
+    }
+    herm_ado<LOGD, PAULI>(a, n, u, rho, out, alpha, base_kind);
+}
+
+// Shared memory of herm_kernel (the operator table sV is reserved in both
+// forms; the PAULI form leaves it unused).
+template <int LOGD>
+size_t herm_smem(int M, int J)
+{
+    const size_t D = size_t(1) << LOGD;
+    const size_t P = (D / 2) * (D + 1);
+    return (D * D + P) * sizeof(double2) + 16 + sizeof(double) * (J * D + LOGD + 4 * M) +
+           sizeof(int) * (4 * M + J);
+}
+
+template <int LOGD, bool PAULI>
+bool prepare_herm_t(int M, int J)
+{
+    const size_t smem = herm_smem<LOGD>(M, J);
+    if (smem > 227 * 1024) return false;
+    static size_t configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && configured[dev] < smem) {
+        if (cudaFuncSetAttribute(herm_kernel<LOGD, PAULI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)) != cudaSuccess)
+            return false;
+        configured[dev] = smem;
+    }
+    return true;
+}
+
+template <int LOGD>
+bool prepare_herm(int M, int J)
+{
+    return prepare_herm_t<LOGD, true>(M, J) && prepare_herm_t<LOGD, false>(M, J);
+}
+
+template <int LOGD>
+bool launch_herm(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha, int base,
+                 cudaStream_t s)
+{
+    if (!prepare_herm<LOGD>(a.M, a.J)) return false;
+    const size_t smem = herm_smem<LOGD>(a.M, a.J);
+    const unsigned grid = static_cast<unsigned>(a.H);
+    if (a.pauli)
+        herm_kernel<LOGD, true><<<grid, HermShape<LOGD>::T, smem, s>>>(a, u, rho, out, alpha, base);
+    else
+        herm_kernel<LOGD, false><<<grid, HermShape<LOGD>::T, smem, s>>>(a, u, rho, out, alpha, base);
+    return true;
+}
+
 template <int LOGD>
 size_t fused_smem(int M, int J)
 {
@@ -380,6 +653,13 @@ __global__ void diag_table_kernel(const double* hdiag, const double* vdiag, cons
 bool launch_fused(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
                    int base_kind, cudaStream_t s)
 {
+    if (a.herm) {
+        switch (a.logd) {
+        case 5: return launch_herm<5>(a, u, rho, out, alpha, base_kind, s);
+        case 6: return launch_herm<6>(a, u, rho, out, alpha, base_kind, s);
+        default: return false;
+        }
+    }
     switch (a.logd) {
     case 5: return launch3<5, 3>(a, u, rho, out, alpha, base_kind, s);
     case 6: return launch3<6, 2>(a, u, rho, out, alpha, base_kind, s);
@@ -387,19 +667,19 @@ bool launch_fused(const FusedArgs& a, const double2* u, const double2* rho, doub
     }
 }
 
-bool prepare_fused(int logd, int M, int J)
+bool prepare_fused(int logd, int M, int J, int herm)
 {
     switch (logd) {
-    case 5: return prepare3<5, 3>(M, J);
-    case 6: return prepare3<6, 2>(M, J);
+    case 5: return herm ? prepare_herm<5>(M, J) : prepare3<5, 3>(M, J);
+    case 6: return herm ? prepare_herm<6>(M, J) : prepare3<6, 2>(M, J);
     default: return false;
     }
 }
 
-bool fused_supported(int logd, int M, int J)
+bool fused_supported(int logd, int M, int J, int herm)
 {
-    if (logd == 5) return fused_smem<5>(M, J) <= 227 * 1024;
-    if (logd == 6) return fused_smem<6>(M, J) <= 227 * 1024;
+    if (logd == 5) return (herm ? herm_smem<5>(M, J) : fused_smem<5>(M, J)) <= 227 * 1024;
+    if (logd == 6) return (herm ? herm_smem<6>(M, J) : fused_smem<6>(M, J)) <= 227 * 1024;
     return false;
 }
 

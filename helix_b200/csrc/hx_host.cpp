@@ -151,6 +151,16 @@ uint64_t binom_u64(int n, int k)
     return static_cast<uint64_t>(r);
 }
 
+int pauli_spin(const double* v, int D)
+{
+    for (int p = 0; (1 << p) < D; ++p) {
+        bool ok = true;
+        for (int r = 0; r < D && ok; ++r) ok = v[r] == (((r >> p) & 1) ? 1.0 : -1.0);
+        if (ok) return p;
+    }
+    return -1;
+}
+
 }  // namespace hx
 
 // ---------------------------------------------------------------------------

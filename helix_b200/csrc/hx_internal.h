@@ -49,6 +49,10 @@ bool bath_constants(double beta, double gamma, double zeta, int K, BathConst& ou
 
 uint64_t binom_u64(int n, int k);
 
+// Spin p when v (d values) is sigma_z of spin p, i.e. v[r] = +1 where bit p
+// of r is set and -1 elsewhere; -1 for any other diagonal.
+int pauli_spin(const double* v, int D);
+
 // ---------------------------------------------------------------------------
 // Device-side parameter blocks
 // ---------------------------------------------------------------------------
@@ -78,6 +82,41 @@ struct StageTables {
 
 enum BaseKind : int { kBaseSelf = 0, kBaseRho = 1, kBaseZero = 2 };
 
+// Hermitian-packed slab.  Every ADO of this hierarchy stays Hermitian: H and
+// the V_j are Hermitian, every commutator term carries a factor -i times a
+// real weight and every anti-commutator term a real weight, so L maps
+// Hermitian matrices to Hermitian matrices, and the initial state is
+// Hermitian.  A packed slab keeps the upper triangle r <= c of a d x d
+// Hermitian matrix (d = 2^logd >= 2) as d/2 packed rows of d + 1 elements:
+// packed row s holds row s from the diagonal on (d - s elements), then row
+// d-1-s from the diagonal on (s + 1 elements).  Consecutive packed elements
+// are consecutive columns of at most two matrix rows, and d(d+1)/2 elements
+// replace d^2.
+__host__ __device__ inline int herm_elems(int logd) { return (1 << (logd - 1)) * ((1 << logd) + 1); }
+// Packed position of element (r, c), r <= c.
+__host__ __device__ inline int herm_index(int r, int c, int logd)
+{
+    const int D = 1 << logd;
+    return r < (D >> 1) ? r * (D + 1) + (c - r) : (D - 1 - r) * (D + 1) + c + 1;
+}
+// Element (r, c), r <= c, at packed position i.
+__host__ __device__ inline void herm_coords(int i, int logd, int& r, int& c)
+{
+    const int D = 1 << logd;
+    const int s = i / (D + 1), t = i - s * (D + 1);
+    if (t < D - s) {
+        r = s;
+        c = s + t;
+    } else {
+        r = D - 1 - s;
+        c = t - 1;
+    }
+}
+// Packed copy of a full d x d table (upper triangle).
+void launch_pack_herm(const double2* full, int logd, double2* packed, cudaStream_t s);
+// Full row-major complex matrix (2 d^2 doubles) from a packed slab, on the host.
+void unpack_herm_host(const double2* pk, int logd, double* out);
+
 // out_n = base_n + alpha * L(u)_n for every ADO n
 void launch_stage(const StageTables& t, const double2* u, const double2* rho, double2* out,
                   double alpha, int base_kind, cudaStream_t s);
@@ -100,9 +139,12 @@ struct FusedArgs {
     int* error_flag;
     long long H;
     int M, J, logd;
+    int herm;                // 1: slabs Hermitian-packed (herm_elems(logd) elements), diag and U packed too
+    const int* vbit;         // [J] spin of V_j = sigma_z(spin) for every bath (pauli = 1), else nullptr
+    int pauli;
 };
-bool fused_supported(int logd, int M, int J);
-bool prepare_fused(int logd, int M, int J);  // raises the shared-memory limit; call before stream capture
+bool fused_supported(int logd, int M, int J, int herm);
+bool prepare_fused(int logd, int M, int J, int herm);  // raises the shared-memory limit; call before stream capture
 bool launch_fused(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
                   int base_kind, cudaStream_t s);
 void launch_entries(const int32_t* rows, const int32_t* edges, const double* acoef, const double* bcoef,
@@ -119,6 +161,7 @@ struct UpTermArgs {
     const int32_t* bath;    // [S][M]
     const int32_t* bath_off;// [J+1]
     int S, M, J, logd;
+    int herm;               // 1: slabs and U Hermitian-packed
 };
 void launch_upterm(const UpTermArgs& a, const double2* u, double2* U, cudaStream_t s);
 
@@ -223,11 +266,13 @@ void launch_coefficients(const int32_t* rows, long long H, int M, int J, const i
 
 // Observables of rho_0: energy = Re Tr(H rho_0), trace.  Optionally copies
 // rho_0 into rho0_copy.  out[0] = energy, out[1] = Re tr, out[2] = Im tr.
-void launch_observables(const double2* rho0, int logd, const double* hdiag, const double* hflip,
+// herm = 1: rho0 is a Hermitian-packed slab.
+void launch_observables(const double2* rho0, int logd, int herm, const double* hdiag, const double* hflip,
                         double2* rho0_copy, double* out, cudaStream_t s);
 
 void launch_finite_check(const double2* x, long long n, int* flag, cudaStream_t s);
-void launch_init_state(double2* rho, long long n, int d, cudaStream_t s);
+// Zero n elements, then rho[one] = 1 (the |d-1><d-1| element of ADO 0).
+void launch_init_state(double2* rho, long long n, long long one, cudaStream_t s);
 
 }  // namespace hx
 
@@ -239,7 +284,9 @@ struct hx_ctx {
     long long H = 0;
     double dt = 0.0;
     uint64_t steps_done = 0;
-    size_t slab = 0;   // d*d
+    size_t slab = 0;   // d*d: elements of one slab as read and written through the C ABI
+    bool herm = false; // state buffers hold Hermitian-packed slabs (fused path, d = 32, 64)
+    size_t slab_store = 0; // elements of one slab in the device buffers (d*d, or herm_elems(logd))
     // device memory
     double2* rho = nullptr;
     double2* ua = nullptr;
@@ -280,6 +327,8 @@ struct hx_ctx {
     int32_t* up_bath = nullptr;   // [S][M]
     double2* U = nullptr;         // [S][d*d]
     double2* diag_table = nullptr;
+    double2* diag_herm = nullptr; // packed diagonal table (herm)
+    int* vbit = nullptr;          // [J] sigma_z spin of each coupling operator, when every one is a sigma_z
     int* ent_count = nullptr;
     int32_t* ent_slab = nullptr;
     int32_t* ent_bath = nullptr;

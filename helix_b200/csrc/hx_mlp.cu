@@ -281,34 +281,46 @@ __global__ void gather_closure_kernel(const float2* __restrict__ din, const floa
         Xb[c] = __float2bfloat16(c - 2 * d2 == k ? 1.f : 0.f);
 }
 
-// Copy, from a fine hierarchy's state, the coarse top-tier ADOs and their up neighbours (FP32).
+// Element e = r d + c of a stored slab: full, or Hermitian-packed (lower
+// triangle read as the conjugate of the upper one).
+__device__ __forceinline__ double2 slab_elem(const double2* slab, int e, int logd, int herm)
+{
+    if (!herm) return slab[e];
+    const int r = e >> logd, c = e & ((1 << logd) - 1);
+    if (r <= c) return slab[herm_index(r, c, logd)];
+    const double2 v = slab[herm_index(c, r, logd)];
+    return make_double2(v.x, -v.y);
+}
+
+// Copy, from a fine hierarchy's state, the coarse top-tier ADOs and their up
+// neighbours (FP32, full d x d); stride = stored elements per slab.
 __global__ void harvest_kernel(const double2* __restrict__ fine, const int* __restrict__ top_fine,
-                               const int* __restrict__ up_fine, int n_top, int n_up, int d2, float2* din,
-                               float2* dout)
+                               const int* __restrict__ up_fine, int n_top, int n_up, int d2, int logd, int herm,
+                               long long stride, float2* din, float2* dout)
 {
     const int s = blockIdx.y;  // slab number: [0, n_top) top tier, then [0, n_up) up neighbours
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= d2) return;
     if (s < n_top) {
-        const double2 v = fine[static_cast<long long>(top_fine[s]) * d2 + e];
+        const double2 v = slab_elem(fine + top_fine[s] * stride, e, logd, herm);
         din[static_cast<long long>(s) * d2 + e] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
     } else {
         const int t = s - n_top;
-        const double2 v = fine[static_cast<long long>(up_fine[t]) * d2 + e];
+        const double2 v = slab_elem(fine + up_fine[t] * stride, e, logd, herm);
         dout[static_cast<long long>(t) * d2 + e] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
     }
 }
 
 // Closure input rows from the coarse state u: row (i, k) = [u_{top i} / s_in, one-hot k].
 __global__ void closure_input_kernel(const double2* __restrict__ u, const int* __restrict__ top, int n_top, int M,
-                                     int d2, float inv_in, int in_ld, bf16* X)
+                                     int d2, int logd, int herm, long long stride, float inv_in, int in_ld, bf16* X)
 {
     const int row = blockIdx.x;  // i * M + k
     const int i = row / M, k = row % M;
-    const double2* ui = u + static_cast<long long>(top[i]) * d2;
+    const double2* ui = u + top[i] * stride;
     bf16* Xb = X + static_cast<long long>(row) * in_ld;
     for (int e = threadIdx.x; e < d2; e += blockDim.x) {
-        const double2 v = ui[e];
+        const double2 v = slab_elem(ui, e, logd, herm);
         Xb[2 * e] = __float2bfloat16(static_cast<float>(v.x) * inv_in);
         Xb[2 * e + 1] = __float2bfloat16(static_cast<float>(v.y) * inv_in);
     }
@@ -316,10 +328,14 @@ __global__ void closure_input_kernel(const double2* __restrict__ u, const int* _
         Xb[c] = __float2bfloat16(c - 2 * d2 == k ? 1.f : 0.f);
 }
 
-// out_{top i} += alpha sum_k -i (v_{j(k)}(r) - v_{j(k)}(c)) (s_out Y_{i,k})   (the dropped up coupling)
+// out_{top i} += alpha sum_k -i (v_{j(k)}(r) - v_{j(k)}(c)) (s_out Yh_{i,k})   (the dropped up coupling),
+// Yh = (Y + Y^H) / 2: the dropped ADO is Hermitian, so the prediction is
+// projected onto its Hermitian part, which keeps the state Hermitian; a
+// Hermitian-packed output takes the upper triangle.
 __global__ void closure_add_kernel(const float* __restrict__ Y, const int* __restrict__ top,
                                    const int* __restrict__ mode_bath, const double* __restrict__ vdiag, int n_top,
-                                   int M, int logd, double s_out, double alpha, double2* out)
+                                   int M, int logd, int herm, long long stride, double s_out, double alpha,
+                                   double2* out)
 {
     const int D = 1 << logd;
     const int d2 = D * D;
@@ -327,17 +343,19 @@ __global__ void closure_add_kernel(const float* __restrict__ Y, const int* __res
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= d2 || i >= n_top) return;
     const int r = e >> logd, c = e & (D - 1);
+    if (herm && r > c) return;
     double sr = 0.0, si = 0.0;
     for (int k = 0; k < M; ++k) {
         const int j = mode_bath[k];
         const double del = vdiag[j * D + r] - vdiag[j * D + c];
         if (del == 0.0) continue;
         const float* y = Y + (static_cast<long long>(i) * M + k) * 2 * d2;
-        sr += del * y[2 * e];
-        si += del * y[2 * e + 1];
+        const int et = (c << logd) + r;  // transposed element
+        sr += del * (0.5 * (static_cast<double>(y[2 * e]) + y[2 * et]));
+        si += del * (0.5 * (static_cast<double>(y[2 * e + 1]) - y[2 * et + 1]));
     }
     // -i del Y = del (Y.y - i Y.x)
-    double2* o = out + static_cast<long long>(top[i]) * d2 + e;
+    double2* o = out + top[i] * stride + (herm ? herm_index(r, c, logd) : e);
     o->x += alpha * s_out * si;
     o->y -= alpha * s_out * sr;
 }
@@ -563,12 +581,14 @@ int closure_stage(hx_closure* cl, const ::hx_ctx* c, const double2* u, double2* 
     hx_mlp* n = cl->net;
     int rc = mlp_reserve(n, rows);
     if (rc != HX_OK) return rc;
-    closure_input_kernel<<<rows, 256, 0, s>>>(u, cl->top_coarse, cl->n_top, cl->M, cl->d2,
+    const int herm = c->herm ? 1 : 0;
+    const long long stride = static_cast<long long>(c->slab_store);
+    closure_input_kernel<<<rows, 256, 0, s>>>(u, cl->top_coarse, cl->n_top, cl->M, cl->d2, cl->logd, herm, stride,
                                               static_cast<float>(1.0 / cl->s_in), n->in_ld, n->X);
     mlp_forward(n, rows, s);
     dim3 grid((cl->d2 + 255) / 256, cl->n_top);
     closure_add_kernel<<<grid, 256, 0, s>>>(n->Y, cl->top_coarse, cl->mode_bath_d, c->vdiag, cl->n_top, cl->M,
-                                           cl->logd, cl->s_out, alpha, out);
+                                           cl->logd, herm, stride, cl->s_out, alpha, out);
     return HX_OK;
 }
 }  // namespace hx
@@ -877,7 +897,8 @@ int hx_closure_harvest(hx_closure* c, hx_ctx* fine)
     const long long snap = c->n_snap;
     dim3 grid((c->d2 + 255) / 256, c->n_top + c->n_up);
     hx::harvest_kernel<<<grid, 256, 0, s>>>(static_cast<const double2*>(state), c->top_fine, c->up_fine, c->n_top,
-                                           c->n_up, c->d2, c->din + snap * c->n_top * c->d2,
+                                           c->n_up, c->d2, c->logd, fine->herm ? 1 : 0,
+                                           static_cast<long long>(fine->slab_store), c->din + snap * c->n_top * c->d2,
                                            c->dout + snap * c->n_up * c->d2);
     HX_CUDA_TRY(cudaGetLastError());
     HX_CUDA_TRY(cudaStreamSynchronize(s));

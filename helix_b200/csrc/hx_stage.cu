@@ -237,21 +237,30 @@ void launch_stage_t(const StageTables& t, const double2* u, const double2* rho, 
     stage_kernel<LOGD><<<static_cast<unsigned>(t.H), threads, smem, s>>>(t, u, rho, out, alpha, base_kind);
 }
 
-__global__ void observables_kernel(const double2* __restrict__ rho0, int logd, const double* __restrict__ hdiag,
-                                   const double* __restrict__ hflip, double2* rho0_copy, double* out)
+// Position of element (r, c) of rho0; in a packed slab the real part of
+// (r, c) equals that of (c, r), which is all the energy needs.
+__device__ __forceinline__ int obs_index(int r, int c, int logd, int herm)
+{
+    if (!herm) return (r << logd) + c;
+    return r <= c ? herm_index(r, c, logd) : herm_index(c, r, logd);
+}
+
+__global__ void observables_kernel(const double2* __restrict__ rho0, int logd, int herm,
+                                   const double* __restrict__ hdiag, const double* __restrict__ hflip,
+                                   double2* rho0_copy, double* out)
 {
     const int D = 1 << logd;
-    const int D2 = D * D;
+    const int n = herm ? herm_elems(logd) : D * D;
     double en = 0.0, tr = 0.0, ti = 0.0;
     for (int r = threadIdx.x; r < D; r += blockDim.x) {
-        const double2 dgl = rho0[r * D + r];
+        const double2 dgl = rho0[obs_index(r, r, logd, herm)];
         en += hdiag[r] * dgl.x;
         tr += dgl.x;
         ti += dgl.y;
-        for (int i = 0; i < logd; ++i) en += hflip[i] * rho0[(r ^ (1 << i)) * D + r].x;
+        for (int i = 0; i < logd; ++i) en += hflip[i] * rho0[obs_index(r ^ (1 << i), r, logd, herm)].x;
     }
     if (rho0_copy)
-        for (int e = threadIdx.x; e < D2; e += blockDim.x) rho0_copy[e] = rho0[e];
+        for (int e = threadIdx.x; e < n; e += blockDim.x) rho0_copy[e] = rho0[e];
     __shared__ double red[3][32];
     for (int off = 16; off > 0; off >>= 1) {
         en += __shfl_down_sync(0xffffffffu, en, off);
@@ -281,11 +290,20 @@ __global__ void finite_kernel(const double2* __restrict__ x, long long n, int* f
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
 }
 
-__global__ void init_state_kernel(double2* rho, long long n, int d)
+__global__ void init_state_kernel(double2* rho, long long n, long long one)
 {
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<long long>(gridDim.x) * blockDim.x)
-        rho[i] = make_double2(i == static_cast<long long>(d) * d - 1 ? 1.0 : 0.0, 0.0);
+        rho[i] = make_double2(i == one ? 1.0 : 0.0, 0.0);
+}
+
+__global__ void pack_herm_kernel(const double2* __restrict__ full, int logd, double2* __restrict__ packed)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= herm_elems(logd)) return;
+    int r, c;
+    herm_coords(i, logd, r, c);
+    packed[i] = full[(r << logd) + c];
 }
 
 }  // namespace
@@ -304,10 +322,16 @@ void launch_stage(const StageTables& t, const double2* u, const double2* rho, do
     }
 }
 
-void launch_observables(const double2* rho0, int logd, const double* hdiag, const double* hflip,
+void launch_observables(const double2* rho0, int logd, int herm, const double* hdiag, const double* hflip,
                         double2* rho0_copy, double* out, cudaStream_t s)
 {
-    observables_kernel<<<1, 256, 0, s>>>(rho0, logd, hdiag, hflip, rho0_copy, out);
+    observables_kernel<<<1, 256, 0, s>>>(rho0, logd, herm, hdiag, hflip, rho0_copy, out);
+}
+
+void launch_pack_herm(const double2* full, int logd, double2* packed, cudaStream_t s)
+{
+    const int n = herm_elems(logd);
+    pack_herm_kernel<<<(n + 255) / 256, 256, 0, s>>>(full, logd, packed);
 }
 
 void launch_finite_check(const double2* x, long long n, int* flag, cudaStream_t s)
@@ -315,9 +339,9 @@ void launch_finite_check(const double2* x, long long n, int* flag, cudaStream_t 
     finite_kernel<<<148 * 4, 256, 0, s>>>(x, n, flag);
 }
 
-void launch_init_state(double2* rho, long long n, int d, cudaStream_t s)
+void launch_init_state(double2* rho, long long n, long long one, cudaStream_t s)
 {
-    init_state_kernel<<<148 * 4, 256, 0, s>>>(rho, n, d);
+    init_state_kernel<<<148 * 4, 256, 0, s>>>(rho, n, one);
 }
 
 }  // namespace hx

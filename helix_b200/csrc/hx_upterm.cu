@@ -28,37 +28,63 @@ constexpr int kTile = 32;          // elements per tile (one per lane)
 // (top-tier count x 512 B per tile) stays in L2.  Every mode of a tier L-1
 // ADO has its up neighbour in the top tier and the up weight -i delta_j is
 // the same for all modes of bath j, so each bath's neighbour slabs are summed
-// unweighted and -i delta_j is applied once.
+// unweighted and -i delta_j is applied once.  A warp sums its slots side by
+// side, so each mode issues kSlotsPerWarp independent loads.
 __device__ __forceinline__ void upterm_block(const UpTermArgs& a, int bx, int by, const double2* __restrict__ u,
                                              double2* __restrict__ U)
 {
     const int D = 1 << a.logd;
-    const long long D2 = static_cast<long long>(D) * D;
+    // elements per stored slab: d^2, or the packed upper triangle
+    const long long D2 = a.herm ? herm_elems(a.logd) : static_cast<long long>(D) * D;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const long long e = static_cast<long long>(by) * kTile + lane;
-    const int r = static_cast<int>(e >> a.logd);
-    const int c = static_cast<int>(e & (D - 1));
+    if (e >= D2) return;
+    int r, c;
+    if (a.herm) {
+        herm_coords(static_cast<int>(e), a.logd, r, c);
+    } else {
+        r = static_cast<int>(e >> a.logd);
+        c = static_cast<int>(e & (D - 1));
+    }
     const double2* ue = u + e;
     const int s0 = (bx * kWarps + warp) * kSlotsPerWarp;
-    for (int s = s0; s < s0 + kSlotsPerWarp && s < a.S; ++s) {
-        const int32_t* slab = a.slab + static_cast<long long>(s) * a.M;
-        double re = 0.0, im = 0.0;
-        for (int j = 0; j < a.J; ++j) {
-            const double del = __ldg(a.vdiag + j * D + r) - __ldg(a.vdiag + j * D + c);
-            if (del == 0.0) continue;
-            const int m1 = __ldg(a.bath_off + j + 1);
-            double sr = 0.0, si = 0.0;
-            for (int m = __ldg(a.bath_off + j); m < m1; ++m) {
-                const double2 y = __ldg(ue + static_cast<long long>(__ldg(slab + m)) * D2);
-                sr += y.x;
-                si += y.y;
+    int ns = a.S - s0;
+    if (ns <= 0) return;
+    ns = ns < kSlotsPerWarp ? ns : kSlotsPerWarp;
+    const int32_t* slab[kSlotsPerWarp];
+#pragma unroll
+    for (int t = 0; t < kSlotsPerWarp; ++t) slab[t] = a.slab + static_cast<long long>(s0 + (t < ns ? t : 0)) * a.M;
+    double re[kSlotsPerWarp], im[kSlotsPerWarp];
+#pragma unroll
+    for (int t = 0; t < kSlotsPerWarp; ++t) re[t] = im[t] = 0.0;
+    for (int j = 0; j < a.J; ++j) {
+        const double del = __ldg(a.vdiag + j * D + r) - __ldg(a.vdiag + j * D + c);
+        if (del == 0.0) continue;
+        const int m1 = __ldg(a.bath_off + j + 1);
+        double sr[kSlotsPerWarp], si[kSlotsPerWarp];
+#pragma unroll
+        for (int t = 0; t < kSlotsPerWarp; ++t) sr[t] = si[t] = 0.0;
+        for (int m = __ldg(a.bath_off + j); m < m1; ++m) {
+            double2 y[kSlotsPerWarp];
+#pragma unroll
+            for (int t = 0; t < kSlotsPerWarp; ++t)
+                y[t] = t < ns ? __ldg(ue + static_cast<long long>(__ldg(slab[t] + m)) * D2) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int t = 0; t < kSlotsPerWarp; ++t) {
+                sr[t] += y[t].x;
+                si[t] += y[t].y;
             }
-            re += del * si;  // -i del S
-            im -= del * sr;
         }
-        U[static_cast<long long>(s) * D2 + e] = make_double2(re, im);
+#pragma unroll
+        for (int t = 0; t < kSlotsPerWarp; ++t) {
+            re[t] += del * si[t];  // -i del S
+            im[t] -= del * sr[t];
+        }
     }
+#pragma unroll
+    for (int t = 0; t < kSlotsPerWarp; ++t)
+        if (t < ns) U[static_cast<long long>(s0 + t) * D2 + e] = make_double2(re[t], im[t]);
 }
 
 __global__ void __launch_bounds__(kWarps * 32)
@@ -126,9 +152,9 @@ __global__ void upterm_tables_kernel(const int32_t* rows, const int32_t* edges, 
 void launch_upterm(const UpTermArgs& a, const double2* u, double2* U, cudaStream_t s)
 {
     if (a.S <= 0) return;
-    const long long D2 = 1ll << (2 * a.logd);
+    const long long D2 = a.herm ? herm_elems(a.logd) : 1ll << (2 * a.logd);
     const int per_cta = kWarps * kSlotsPerWarp;
-    dim3 grid((a.S + per_cta - 1) / per_cta, static_cast<unsigned>(D2 / kTile));  // d >= 32: D2 % 32 == 0
+    dim3 grid((a.S + per_cta - 1) / per_cta, static_cast<unsigned>((D2 + kTile - 1) / kTile));
     upterm_kernel<<<grid, kWarps * 32, 0, s>>>(a, u, U);
 }
 

@@ -80,14 +80,23 @@ typedef struct hx_problem {
     double time_step;           /* dt (Param::Step) */
     uint32_t integration_order; /* Taylor order (Param::IntegrationNum), 1..8 */
     uint32_t precision;         /* HX_PRECISION_DOUBLE or HX_PRECISION_MIXED */
-    uint32_t flags;             /* reserved, 0 */
+    uint32_t flags;             /* 0 or HX_FLAG_FULL_STATE */
 } hx_problem;
+
+/* Every ADO of this hierarchy stays Hermitian (H and the V_j are Hermitian
+ * and every term of the right-hand side maps Hermitian matrices to Hermitian
+ * matrices), so for d = 32 and 64 the device state keeps the upper triangle
+ * of each slab only (d(d+1)/2 elements instead of d^2), which halves the
+ * memory traffic of a step.  The C ABI still reads and writes full d x d
+ * slabs; hx_ctx_write_state then rejects non-Hermitian ADOs.  This flag keeps
+ * full slabs on the device, for general (non-Hermitian) states. */
+#define HX_FLAG_FULL_STATE 1u
 
 typedef struct hx_info {
     uint32_t dim;
     uint32_t modes;
     uint64_t hierarchy_size;    /* number of ADOs */
-    uint64_t state_bytes;       /* bytes of one full hierarchy state */
+    uint64_t state_bytes;       /* device bytes of one hierarchy state (packed slabs count d(d+1)/2) */
     uint64_t device_bytes;      /* device memory the context holds */
     uint64_t steps_done;
     double time;                /* steps_done * dt */
@@ -192,7 +201,10 @@ int hx_ctx_write_state(hx_ctx* ctx, const double* in, uint64_t n);
 
 /* Device pointer of the state (hierarchy_size * d * d double2), for callers
  * that fill or read it on the device.  In mixed precision this is the
- * double-precision slab of ADO 0 only (d * d double2). */
+ * double-precision slab of ADO 0 only (d * d double2).  With Hermitian-packed
+ * slabs (d = 32, 64 without HX_FLAG_FULL_STATE) each slab holds d(d+1)/2
+ * double2: element (r, c), r <= c, at r*(d+1) + c - r when r < d/2, else at
+ * (d-1-r)*(d+1) + c + 1. */
 int hx_ctx_state_device_ptr(hx_ctx* ctx, void** ptr);
 
 /* One evaluation of the right-hand side L(rho) of the current state into a

@@ -77,3 +77,32 @@ def test_last_error_text_is_thread_local_string():
     except capi.HxError as e:
         assert "mode" in str(e)
     assert isinstance(capi.lib().hx_last_error(), bytes)
+
+
+@pytest.mark.parametrize("d", [2, 4, 8, 32, 64])
+def test_hermitian_packed_layout_is_a_bijection(d):
+    """herm_index maps the upper triangle one-to-one onto 0..d(d+1)/2-1 and
+    unpack_herm inverts it (the documented device layout of packed slabs)."""
+    P = d * (d + 1) // 2
+    seen = np.full(P, -1)
+    for r in range(d):
+        for c in range(r, d):
+            i = capi.herm_index(r, c, d)
+            assert 0 <= i < P and seen[i] == -1
+            seen[i] = r * d + c
+    rng = np.random.default_rng(d)
+    x = rng.standard_normal((3, d, d)) + 1j * rng.standard_normal((3, d, d))
+    x = x + np.conj(np.transpose(x, (0, 2, 1)))
+    packed = np.stack([[x[k, r, c] for r in range(d) for c in range(r, d)] for k in range(3)])
+    order = np.array([capi.herm_index(r, c, d) for r in range(d) for c in range(r, d)])
+    pk = np.zeros((3, P), np.complex128)
+    pk[:, order] = packed
+    np.testing.assert_array_equal(capi.unpack_herm(pk, d), x)
+
+
+def test_full_state_flag_is_the_only_flag():
+    p = S.spin_glass(2, seed=1, depth=2, K=1)
+    prob, keep = capi._problem_struct(p, flags=2)
+    h = C.c_void_p()
+    rc = capi.lib().hx_ctx_create(C.byref(prob), C.byref(h))
+    assert rc == 6 and "flags" in capi.lib().hx_last_error().decode()  # InvalidRuntimeOption, no device call

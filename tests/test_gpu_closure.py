@@ -100,3 +100,39 @@ def test_closure_beats_truncation_on_held_out_seeds():
     # trained closure must cut it by a factor of 1.5 or more
     assert min(gains) > 1.5, gains
     cl.close()
+
+
+def test_closure_on_packed_and_full_slabs_agree():
+    """At d = 32 the contexts keep Hermitian-packed slabs; the closure reads
+    (harvest, input rows) and writes (closure term) them through the packed
+    layout.  Harvesting from a packed or a full-slab fine hierarchy and
+    attaching to a packed or a full-slab coarse one give the same numbers."""
+    n, K, steps = 5, 1, 40
+    coarse = S.spin_glass(n, seed=31, depth=2, K=K, h=1.0, dt=0.005)
+    fine = S.spin_glass(n, seed=31, depth=3, K=K, h=1.0, dt=0.005)
+    made = []
+    for full in (False, True):
+        cl = capi.Closure(coarse, fine_max_depth=4, hidden=64, capacity=4, seed=3)
+        with capi.Context(fine, full_state=full) as ctx:
+            assert ctx.hermitian_packed != full
+            for _ in range(4):
+                ctx.step(10)
+                cl.harvest(ctx)
+        cl.train(iters=50, batch=64, lr=1e-3, seed=5)
+        made.append(cl)
+    # the two training sets agree (their RMS scales, to rounding of the
+    # independently computed lower triangles of the full-slab run)
+    a, b = made[0].info(), made[1].info()
+    assert a["snapshots"] == b["snapshots"] == 4
+    assert abs(a["s_in"] - b["s_in"]) <= 1e-6 * b["s_in"] and abs(a["s_out"] - b["s_out"]) <= 1e-6 * b["s_out"]
+    trajs = []
+    for full in (False, True):
+        with capi.Context(coarse, full_state=full) as ctx:
+            made[0].attach(ctx)
+            rho, _ = ctx.step_trace(steps, rho0=True, energy=False)
+            trajs.append(rho)
+    assert np.max(np.abs(trajs[0] - trajs[1])) <= 1e-10
+    plain = _rho_traj(coarse, steps)
+    assert np.max(np.abs(trajs[0] - plain)) > 1e-8  # the closure term is there
+    for cl in made:
+        cl.close()

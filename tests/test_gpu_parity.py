@@ -48,19 +48,25 @@ def test_device_tables_random_shapes_vs_oracle():
         np.testing.assert_array_equal(e1, e2)
 
 
-def _random_state(size, d, seed):
+def _random_state(size, d, seed, hermitian=False):
     rng = np.random.default_rng(seed)
     x = rng.standard_normal((size, d, d)) + 1j * rng.standard_normal((size, d, d))
+    if hermitian:
+        x = 0.5 * (x + np.conj(np.transpose(x, (0, 2, 1))))
     return x.astype(np.complex128)
 
 
+@pytest.mark.parametrize("state", ["hermitian", "general"])
 @pytest.mark.parametrize("n,K,depth", [(1, 1, 2), (2, 1, 3), (3, 2, 2), (4, 2, 2), (5, 1, 2), (6, 1, 1)])
-def test_rhs_matches_oracle(n, K, depth):
+def test_rhs_matches_oracle(n, K, depth, state):
+    """Hermitian states run on the default layout (Hermitian-packed slabs for
+    d = 32, 64); general states on full slabs (full_state=True)."""
     p = S.spin_glass(n, seed=100 + n, depth=depth, K=K, h=0.7)
     o = O.Oracle(p)
-    with capi.Context(p) as ctx:
+    with capi.Context(p, full_state=state == "general") as ctx:
         assert ctx.size == o.size
-        x = _random_state(ctx.size, p.dim, n)
+        assert ctx.hermitian_packed == (state == "hermitian" and p.dim >= 32)
+        x = _random_state(ctx.size, p.dim, n, hermitian=state == "hermitian")
         ctx.set_state(x)
         got = ctx.rhs()
     want = o.rhs(x)
@@ -137,8 +143,9 @@ def test_c2_full_size_one_step_and_invariants():
     p = S.spin_glass(6, seed=2025, depth=4, K=2, h=1.0, dt=0.005)
     with capi.Context(p) as ctx:
         assert ctx.size == 7315
-        # populate every tier: start from a random Hermitian-ish state
-        x = _random_state(ctx.size, p.dim, 1) * 1e-3
+        assert ctx.hermitian_packed
+        # populate every tier: start from a random Hermitian state
+        x = _random_state(ctx.size, p.dim, 1, hermitian=True) * 1e-3
         x[0] = S.initial_rho0(p.dim)
         ctx.set_state(x)
         ctx.step(1)
@@ -207,20 +214,24 @@ def test_non_finite_state_is_reported():
         assert err.value.status == "NonFiniteState"
 
 
-@pytest.mark.parametrize("variant", ["generic", "fused"])
+@pytest.mark.parametrize("variant", ["generic", "fused", "fused-packed"])
 @pytest.mark.parametrize("n,K,depth", [(5, 2, 2), (6, 2, 2), (6, 1, 3), (5, 1, 0), (6, 2, 1)])
 def test_all_stage_kernels_match_oracle(monkeypatch, variant, n, K, depth):
-    """d = 32 / 64 run the up-term kernel + fused multi-CTA kernel by default;
-    HX_FORCE_GENERIC_STAGE=1 selects the generic one-slab-per-CTA kernel.
-    Both must match the oracle, including depth 0 (no hierarchy) and depth 1
-    (every tier-0 up neighbour handled by the up-term kernel)."""
+    """d = 32 / 64 run the up-term kernel + fused multi-CTA kernel on
+    Hermitian-packed slabs by default ("fused-packed", Hermitian states); with
+    full slabs ("fused", general states); HX_FORCE_GENERIC_STAGE=1 selects the
+    generic one-slab-per-CTA kernel.  All must match the oracle, including
+    depth 0 (no hierarchy) and depth 1 (every tier-0 up neighbour handled by
+    the up-term kernel)."""
     monkeypatch.delenv("HX_FORCE_GENERIC_STAGE", raising=False)
     if variant == "generic":
         monkeypatch.setenv("HX_FORCE_GENERIC_STAGE", "1")
     p = S.spin_glass(n, seed=300 + n, depth=depth, K=K, h=0.8, dt=0.005)
     o = O.Oracle(p)
-    with capi.Context(p) as ctx:
-        x = _random_state(ctx.size, p.dim, 11) * 1e-2
+    packed = variant == "fused-packed"
+    with capi.Context(p, full_state=not packed) as ctx:
+        assert ctx.hermitian_packed == packed
+        x = _random_state(ctx.size, p.dim, 11, hermitian=packed) * 1e-2
         x[0] = S.initial_rho0(p.dim)
         ctx.set_state(x)
         got = ctx.rhs()
@@ -232,3 +243,39 @@ def test_all_stage_kernels_match_oracle(monkeypatch, variant, n, K, depth):
         o.run(3)
         assert np.max(np.abs(ctx.state() - o.state())) <= TOL
     o.close()
+
+
+class _DeviceView:
+    """Zero-copy view of device memory for torch.as_tensor."""
+
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<c16", "data": (ptr, False), "version": 3}
+
+
+@pytest.mark.parametrize("n", [5, 6])
+def test_packed_layout_and_rejection(n):
+    """The device layout of a packed context is the documented one
+    (capi.herm_index / unpack_herm), ADO 0 starts as |d-1><d-1|, and
+    non-Hermitian states are refused with a message naming the flag."""
+    import torch
+
+    p = S.spin_glass(n, seed=9, depth=2, K=1, h=0.5)
+    d = p.dim
+    P = d * (d + 1) // 2
+    with capi.Context(p) as ctx:
+        assert ctx.hermitian_packed and ctx.info.state_bytes == ctx.size * P * 16
+        dev = torch.as_tensor(_DeviceView(ctx.state_device_ptr(), ctx.size * P), device="cuda")
+        packed0 = dev[:P].cpu().numpy()
+        np.testing.assert_array_equal(capi.unpack_herm(packed0, d), S.initial_rho0(d))
+        assert packed0[capi.herm_index(d - 1, d - 1, d)] == 1.0
+        ctx.step(4)
+        ctx.sync()
+        st = ctx.state()
+        np.testing.assert_array_equal(st, np.conj(np.transpose(st, (0, 2, 1))))
+        np.testing.assert_array_equal(capi.unpack_herm(dev.cpu().numpy().reshape(ctx.size, P), d), st)
+        with pytest.raises(capi.HxError) as err:
+            ctx.set_state(_random_state(ctx.size, d, 3))
+        assert err.value.status == "InvalidRuntimeOption" and "HX_FLAG_FULL_STATE" in str(err.value)
+        xh = _random_state(ctx.size, d, 4, hermitian=True)
+        ctx.set_state(xh)
+        np.testing.assert_array_equal(ctx.state(), xh)
