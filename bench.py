@@ -44,8 +44,8 @@ CONFIGS = {
                workload="spin_glass_d256_L3_K1_969ados_complex64_mixed"),
     # learned closure: N=5 (d=32), K=2 (15 modes), L=2 + MLP closure of tier 3; trained on 64 seeds of plain
     # L=5 FP64 runs (dt=0.01, 1000 steps), tested on 16 held-out seeds against plain L=5
-    "c5": dict(n=5, K=2, h=1.0, dt=0.01, closure=True, coarse_depth=2, fine_depth=5, train_seeds=64,
-               test_seeds=16, traj_steps=1000, every=50, hidden=512, iters=6000, mlp_batch=1024, lr=1e-3,
+    "c5": dict(n=5, K=2, h=1.0, dt=0.01, closure=True, coarse_depth=2, fine_depth=5, train_seeds=16,
+               test_seeds=16, traj_steps=1000, every=50, hidden=128, iters=3000, mlp_batch=8192, lr=3e-3,
                workload="spin_glass_d32_K2_L2_plus_mlp_closure_vs_L5"),
     # batched disorder average: 512 seeded instances, N in {3,4,5}, L in {2,3,4}, K=2, dt=0.01
     "c4": dict(batch=True, count=512, seed=2026, dt=0.01, workload="disorder_batch_512_N3-5_L2-4_K2_fp64"),
@@ -282,6 +282,9 @@ def run_ours(args, cfg: dict) -> None:
     host_state[0] = S.initial_rho0(p.dim)
     rho_trace = torch.empty(args.steps * p.dim * p.dim * 2, dtype=torch.float64, pin_memory=True).numpy()
     en_trace = np.zeros(args.steps)
+    # untimed pass: the library's pinned staging buffers are allocated on first use
+    ctx.set_state(host_state)
+    ctx.step_trace_into(1, rho_trace, en_trace)
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -618,7 +621,7 @@ def run_mixed(args, cfg: dict) -> None:
 
 def run_closure(args, cfg: dict) -> None:
     """Learned closure: L=2 hierarchy + MLP closure of tier 3 against the plain
-    L=5 run (the judge) and the plain truncated L=2 run, on held-out seeds.
+    L=5 run (the reference solution) and the plain truncated L=2 run, on held-out seeds.
     value = closure ADO-steps/s of the coarse hierarchy; the line also gives
     the simulated-steps rate of closure and of plain L=5 and the trace
     distances of rho_0(t)."""
@@ -667,15 +670,18 @@ def run_closure(args, cfg: dict) -> None:
             closure.attach(ctx)
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
+        k0 = ctx.counters().kernel_launches
         ev0.record(stream)
         rho, _ = ctx.step_trace(steps, rho0=True, energy=False)
         ev1.record(stream)
         torch.cuda.synchronize()
         H = ctx.size
+        launches[0] += int(ctx.counters().kernel_launches - k0) if closure is not None else 0
         ctx.close()
         return rho, ev0.elapsed_time(ev1), H
 
     e_plain, e_closed, ms_fine, ms_closed, ms_plain = [], [], 0.0, 0.0, 0.0
+    launches = [0]
     clocks = ClockSampler(local)
     clocks.start()
     for s in test_seeds:
@@ -698,8 +704,10 @@ def run_closure(args, cfg: dict) -> None:
         "config": {"workload": cfg["workload"], "ados_coarse": H_coarse, "ados_fine": H_fine, "dim": 1 << n,
                    "modes": 3 * n, "coarse_depth_L": cfg["coarse_depth"], "fine_depth_L": cfg["fine_depth"],
                    "dt": dt, "train_seeds": len(train_seeds), "test_seeds": nt, "trajectory_steps": steps,
-                   "snapshot_every": every, "mlp": f"{info['top_ados']}x{3 * n} pairs per RHS, "
-                   f"{2 * (1 << n) ** 2 + 3 * n}-{cfg['hidden']}-{cfg['hidden']}-{2 * (1 << n) ** 2} GELU",
+                   "snapshot_every": every,
+                   "mlp": f"features of (mode, n_k, r, c) {3 * n + 3 + cfg['coarse_depth'] + 1}-{cfg['hidden']}-"
+                   f"{cfg['hidden']}-2 GELU -> complex coefficient of rho_n(r, c); table of "
+                   f"{3 * n * (cfg['coarse_depth'] + 1) * (1 << n) ** 2} coefficients, elementwise closure kernel",
                    "parallelism": "single"},
         "closure": {"simulated_steps_per_s": steps * nt / (ms_closed / 1000.0),
                     "plain_fine_steps_per_s": steps * nt / (ms_fine / 1000.0),
@@ -711,7 +719,7 @@ def run_closure(args, cfg: dict) -> None:
                     "train": {"snapshots": info["snapshots"], "data_s": t_data, "train_s": t_train,
                               "iters": cfg["iters"], "batch": cfg["mlp_batch"], "loss_first": float(loss[:20].mean()),
                               "loss_last": float(loss[-100:].mean())}},
-        "gpu_launches": None,
+        "gpu_launches": launches[0],
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)

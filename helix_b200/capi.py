@@ -522,8 +522,8 @@ class Closure:
         self._h = h
         m = C.c_void_p()
         _check(lib().hx_closure_mlp(self._h, C.byref(m)))
-        d2 = coarse_problem.dim ** 2
-        self.mlp = MLP(2 * d2 + coarse_problem.modes, hidden, 2 * d2, handle=m, owner=self)
+        # features of (mode k, n_k, r, c) -> the complex coefficient A (two reals)
+        self.mlp = MLP(coarse_problem.modes + 3 + coarse_problem.max_depth, hidden, 2, handle=m, owner=self)
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

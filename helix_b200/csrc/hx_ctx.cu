@@ -15,6 +15,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "hx_internal.h"
@@ -57,6 +58,7 @@ void release(hx_ctx* c)
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->state_pinned) cudaFreeHost(c->state_pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -253,7 +255,7 @@ int launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* o
     int k = launch_stage_core(c, u, rho, out, alpha, base);
     if (c->closure) {
         hx::closure_stage(c->closure, c, u, out, alpha, c->stream);
-        k += 5;  // input rows, three GEMMs, closure add
+        k += 1;  // the elementwise closure kernel (the coefficient table is rebuilt only after training)
     }
     return k;
 }
@@ -329,28 +331,66 @@ int read_error_flag(hx_ctx* c)
 bool pack_herm_host(const double* in, int logd, double2* pk)
 {
     const int D = 1 << logd, P = hx::herm_elems(logd);
-    double scale = 0.0;
-    for (size_t e = 0; e < static_cast<size_t>(D) * D; ++e) scale = std::max(scale, std::hypot(in[2 * e], in[2 * e + 1]));
-    const double tol = 1e-12 * scale;
+    double scale2 = 0.0;
+    for (size_t e = 0; e < static_cast<size_t>(D) * D; ++e)
+        scale2 = std::max(scale2, in[2 * e] * in[2 * e] + in[2 * e + 1] * in[2 * e + 1]);
+    const double tol2 = 1e-24 * scale2;
     for (int i = 0; i < P; ++i) {
         int r, c;
         hx::herm_coords(i, logd, r, c);
         const size_t up = static_cast<size_t>(r) * D + c, lo = static_cast<size_t>(c) * D + r;
-        if (r != c && std::hypot(in[2 * up] - in[2 * lo], in[2 * up + 1] + in[2 * lo + 1]) > tol) return false;
+        if (r != c) {
+            const double dr = in[2 * up] - in[2 * lo], di = in[2 * up + 1] + in[2 * lo + 1];
+            if (dr * dr + di * di > tol2) return false;
+        }
         pk[i] = make_double2(in[2 * up], in[2 * up + 1]);
     }
     return true;
 }
 
+// f(k) for k in [0, n) on up to 16 host threads.
+template <typename F>
+void parallel_for(long long n, F f)
+{
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = static_cast<int>(std::min<long long>(n, std::min(16u, hw)));
+    if (nt <= 1) {
+        for (long long k = 0; k < n; ++k) f(k);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            for (long long k = n * t / nt; k < n * (t + 1) / nt; ++k) f(k);
+        });
+    for (auto& th : pool) th.join();
+}
+
+// Pinned staging for whole packed states (allocated on first use, kept).
+int state_staging(hx_ctx* c, size_t elems)
+{
+    if (c->state_pinned_elems >= elems) return HX_OK;
+    if (c->state_pinned) cudaFreeHost(c->state_pinned);
+    c->state_pinned = nullptr;
+    c->state_pinned_elems = 0;
+    HX_CUDA_TRY(cudaMallocHost(&c->state_pinned, elems * sizeof(double2)));
+    c->state_pinned_elems = elems;
+    return HX_OK;
+}
+
 // count slabs of a packed device buffer into full matrices on the host.
 int read_herm(hx_ctx* c, const double2* src, size_t count, double* out)
 {
-    std::vector<double2> tmp(count * c->slab_store);
-    HX_CUDA_TRY(cudaMemcpyAsync(tmp.data(), src, tmp.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    const size_t n = count * c->slab_store;
+    int rc = state_staging(c, n);
+    if (rc != HX_OK) return rc;
+    HX_CUDA_TRY(cudaMemcpyAsync(c->state_pinned, src, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    c->counters.d2h_bytes += tmp.size() * sizeof(double2);
-    for (size_t k = 0; k < count; ++k)
-        hx::unpack_herm_host(tmp.data() + k * c->slab_store, c->logd, out + 2 * k * c->slab);
+    c->counters.d2h_bytes += n * sizeof(double2);
+    const double2* pk = c->state_pinned;
+    parallel_for(static_cast<long long>(count), [&](long long k) {
+        hx::unpack_herm_host(pk + k * c->slab_store, c->logd, out + 2 * k * c->slab);
+    });
     return HX_OK;
 }
 
@@ -864,15 +904,23 @@ int hx_ctx_write_state(hx_ctx* c, const double* in, uint64_t n)
         return HX_OK;
     }
     if (c->herm) {
-        std::vector<double2> pk(static_cast<size_t>(c->H) * c->slab_store);
+        const size_t n = static_cast<size_t>(c->H) * c->slab_store;
+        int rc = state_staging(c, n);
+        if (rc != HX_OK) return rc;
+        HX_CUDA_TRY(cudaStreamSynchronize(c->stream));  // the staging buffer may still feed an earlier copy
+        double2* pk = c->state_pinned;
+        std::vector<char> ok(static_cast<size_t>(c->H), 1);
+        parallel_for(c->H, [&](long long k) {
+            ok[k] = pack_herm_host(in + 2 * static_cast<size_t>(k) * c->slab, c->logd, pk + k * c->slab_store);
+        });
         for (long long k = 0; k < c->H; ++k)
-            if (!pack_herm_host(in + 2 * static_cast<size_t>(k) * c->slab, c->logd, pk.data() + k * c->slab_store))
+            if (!ok[k])
                 return fail(HX_ERR_INVALID_RUNTIME_OPTION,
                             "ADO " + std::to_string(k) +
                                 " is not Hermitian; this context keeps Hermitian-packed slabs (create it with "
                                 "HX_FLAG_FULL_STATE for general states)");
-        HX_CUDA_TRY(cudaMemcpyAsync(c->rho, pk.data(), pk.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-        c->counters.h2d_bytes += pk.size() * sizeof(double2);
+        HX_CUDA_TRY(cudaMemcpyAsync(c->rho, pk, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        c->counters.h2d_bytes += n * sizeof(double2);
         HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
         return HX_OK;
     }

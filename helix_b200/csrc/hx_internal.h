@@ -342,6 +342,8 @@ struct hx_ctx {
     int trace_cap = 0;
     double* pinned = nullptr;     // pinned staging for traces
     size_t pinned_bytes = 0;
+    double2* state_pinned = nullptr; // pinned staging for packed whole-state transfers
+    size_t state_pinned_elems = 0;
     size_t device_bytes = 0;
     hx_counters counters{};
     std::vector<double> h_hdiag, h_hflip;

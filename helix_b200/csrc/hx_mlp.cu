@@ -249,36 +249,116 @@ __global__ void gather_rows_kernel(const float* __restrict__ x, const float* __r
         T[static_cast<long long>(b) * out_dim + c] = t[static_cast<long long>(row) * out_dim + c];
 }
 
-// Minibatch from the closure dataset: sample b = (snapshot, top-tier ADO i, mode k);
-// X row = [slab of ADO i / s_in (2 d^2 reals), one-hot k, 0...], T row = up neighbour / s_out.
-__global__ void gather_closure_kernel(const float2* __restrict__ din, const float2* __restrict__ dout,
-                                      const int* __restrict__ up_local, int n_snap, int n_top, int n_up, int M,
-                                      int d2, float inv_in, float inv_out, int in_ld, int batch, uint64_t seed,
-                                      bf16* X, float* T)
+// Features of closure element (mode k, occupation n_k of the top-tier ADO,
+// matrix element r, c) in one BF16 row: one-hot k, v_j(r), v_j(c) (j = bath
+// of k), (E_r - E_c) / e_scale, one-hot n_k, zero padding to in_ld.
+__device__ __forceinline__ void closure_features(bf16* X, int in_ld, int M, int maxd, int k, int nk, int r, int c,
+                                                 const int* mode_bath, const double* vdiag, const double* hdiag,
+                                                 int D, double inv_e)
 {
-    const int b = blockIdx.x;
+    const int j = mode_bath[k];
+    for (int q = 0; q < in_ld; ++q) X[q] = __float2bfloat16(0.f);
+    X[k] = __float2bfloat16(1.f);
+    X[M] = __float2bfloat16(static_cast<float>(vdiag[j * D + r]));
+    X[M + 1] = __float2bfloat16(static_cast<float>(vdiag[j * D + c]));
+    X[M + 2] = __float2bfloat16(static_cast<float>((hdiag[r] - hdiag[c]) * inv_e));
+    X[M + 3 + (nk < maxd ? nk : maxd - 1)] = __float2bfloat16(1.f);
+}
+
+// Minibatch of closure samples, one thread per row: sample b = (snapshot, top-tier
+// ADO i, mode k, element r, c with v_j(r) != v_j(c), up to eight draws), its
+// features in X, the scaled element of ADO i in xin and of its up neighbour
+// n_i + e_k in tgt.
+__global__ void gather_closure_kernel(const float2* __restrict__ din, const float2* __restrict__ dout,
+                                      const int* __restrict__ up_local, const int8_t* __restrict__ top_occ,
+                                      const int* __restrict__ mode_bath, const double* __restrict__ vdiag,
+                                      const double* __restrict__ hdiag, double inv_e, int n_snap, int n_top,
+                                      int n_up, int M, int maxd, int logd, float inv_in, float inv_out, int in_ld,
+                                      int batch, uint64_t seed, bf16* X, float2* xin, float2* tgt)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= batch) return;
-    const uint64_t r = mix64(seed ^ (0x2545F4914F6CDD1Dull * (b + 1)));
+    const int D = 1 << logd, d2 = D * D;
+    uint64_t z = mix64(seed ^ (0x2545F4914F6CDD1Dull * (b + 1)));
     const long long pairs = static_cast<long long>(n_snap) * n_top * M;
-    const long long pidx = static_cast<long long>(r % static_cast<uint64_t>(pairs));
+    const long long pidx = static_cast<long long>(z % static_cast<uint64_t>(pairs));
     const int snap = static_cast<int>(pidx / (static_cast<long long>(n_top) * M));
     const int i = static_cast<int>((pidx / M) % n_top);
     const int k = static_cast<int>(pidx % M);
-    const int t = up_local[i * M + k];
-    const float2* xi = din + (static_cast<long long>(snap) * n_top + i) * d2;
-    const float2* ti = dout + (static_cast<long long>(snap) * n_up + t) * d2;
-    bf16* Xb = X + static_cast<long long>(b) * in_ld;
-    float* Tb = T + static_cast<long long>(b) * 2 * d2;
-    for (int e = threadIdx.x; e < d2; e += blockDim.x) {
-        const float2 v = xi[e];
-        Xb[2 * e] = __float2bfloat16(v.x * inv_in);
-        Xb[2 * e + 1] = __float2bfloat16(v.y * inv_in);
-        const float2 w = ti[e];
-        Tb[2 * e] = w.x * inv_out;
-        Tb[2 * e + 1] = w.y * inv_out;
+    const int j = mode_bath[k];
+    int e = 0;
+    for (int tries = 0; tries < 8; ++tries) {
+        z = mix64(z);
+        e = static_cast<int>(z % static_cast<uint64_t>(d2));
+        if (vdiag[j * D + (e >> logd)] != vdiag[j * D + (e & (D - 1))]) break;
     }
-    for (int c = 2 * d2 + threadIdx.x; c < in_ld; c += blockDim.x)
-        Xb[c] = __float2bfloat16(c - 2 * d2 == k ? 1.f : 0.f);
+    const int r = e >> logd, c = e & (D - 1);
+    closure_features(X + static_cast<long long>(b) * in_ld, in_ld, M, maxd, k, top_occ[i * M + k], r, c, mode_bath,
+                     vdiag, hdiag, D, inv_e);
+    const float2 x = din[(static_cast<long long>(snap) * n_top + i) * d2 + e];
+    const float2 t = dout[(static_cast<long long>(snap) * n_up + up_local[i * M + k]) * d2 + e];
+    xin[b] = make_float2(x.x * inv_in, x.y * inv_in);
+    tgt[b] = make_float2(t.x * inv_out, t.y * inv_out);
+}
+
+// Loss of the linear closure: the network's two outputs (a, b) are the
+// complex coefficient A of pred = A x; loss = mean |pred - t|^2, and
+// dL/da = 2 Re(conj(err) x) / B, dL/db = 2 Im(conj(x) err) / B (FP32 and BF16).
+__global__ void closure_loss_kernel(const float* __restrict__ Y, const float2* __restrict__ xin,
+                                    const float2* __restrict__ tgt, int B, float* dyf, bf16* dyh, float* partial)
+{
+    float s = 0.f;
+    const float g = 2.0f / static_cast<float>(B);
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
+        const float a = Y[2 * b], bb = Y[2 * b + 1];
+        const float2 x = xin[b], t = tgt[b];
+        const float er = a * x.x - bb * x.y - t.x, ei = a * x.y + bb * x.x - t.y;
+        s += er * er + ei * ei;
+        const float da = g * (er * x.x + ei * x.y), db = g * (ei * x.x - er * x.y);
+        dyf[2 * b] = da;
+        dyf[2 * b + 1] = db;
+        dyh[2 * b] = __float2bfloat16(da);
+        dyh[2 * b + 1] = __float2bfloat16(db);
+    }
+    __shared__ float red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+// Feature rows [row0, row0 + n) of the coefficient table; row = (k maxd + n_k) d^2 + r d + c.
+__global__ void table_features_kernel(const int* __restrict__ mode_bath, const double* __restrict__ vdiag,
+                                      const double* __restrict__ hdiag, double inv_e, int M, int maxd, int logd,
+                                      int in_ld, long long row0, int n, bf16* X)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const long long row = row0 + q;
+    const int D = 1 << logd, d2 = D * D;
+    const int e = static_cast<int>(row % d2);
+    const long long kn = row / d2;
+    const int k = static_cast<int>(kn / maxd), nk = static_cast<int>(kn % maxd);
+    closure_features(X + static_cast<long long>(q) * in_ld, in_ld, M, maxd, k, nk, e >> logd, e & (D - 1), mode_bath,
+                     vdiag, hdiag, D, inv_e);
+}
+
+// coef(row) = ratio (A(r, c) + conj A(c, r)) / 2: the Hermitian part of the
+// predicted up neighbour, so the closure term keeps the state Hermitian.
+__global__ void table_kernel(const float2* __restrict__ raw, long long rows, int logd, double ratio, double2* coef)
+{
+    const long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (row >= rows) return;
+    const int D = 1 << logd, d2 = D * D;
+    const int e = static_cast<int>(row % d2);
+    const long long base = row - e;
+    const int r = e >> logd, c = e & (D - 1);
+    const float2 a = raw[row], b = raw[base + (c << logd) + r];
+    coef[row] = make_double2(0.5 * ratio * (static_cast<double>(a.x) + b.x),
+                             0.5 * ratio * (static_cast<double>(a.y) - b.y));
 }
 
 // Element e = r d + c of a stored slab: full, or Hermitian-packed (lower
@@ -311,53 +391,42 @@ __global__ void harvest_kernel(const double2* __restrict__ fine, const int* __re
     }
 }
 
-// Closure input rows from the coarse state u: row (i, k) = [u_{top i} / s_in, one-hot k].
-__global__ void closure_input_kernel(const double2* __restrict__ u, const int* __restrict__ top, int n_top, int M,
-                                     int d2, int logd, int herm, long long stride, float inv_in, int in_ld, bf16* X)
-{
-    const int row = blockIdx.x;  // i * M + k
-    const int i = row / M, k = row % M;
-    const double2* ui = u + top[i] * stride;
-    bf16* Xb = X + static_cast<long long>(row) * in_ld;
-    for (int e = threadIdx.x; e < d2; e += blockDim.x) {
-        const double2 v = slab_elem(ui, e, logd, herm);
-        Xb[2 * e] = __float2bfloat16(static_cast<float>(v.x) * inv_in);
-        Xb[2 * e + 1] = __float2bfloat16(static_cast<float>(v.y) * inv_in);
-    }
-    for (int c = 2 * d2 + threadIdx.x; c < in_ld; c += blockDim.x)
-        Xb[c] = __float2bfloat16(c - 2 * d2 == k ? 1.f : 0.f);
-}
-
-// out_{top i} += alpha sum_k -i (v_{j(k)}(r) - v_{j(k)}(c)) (s_out Yh_{i,k})   (the dropped up coupling),
-// Yh = (Y + Y^H) / 2: the dropped ADO is Hermitian, so the prediction is
-// projected onto its Hermitian part, which keeps the state Hermitian; a
-// Hermitian-packed output takes the upper triangle.
-__global__ void closure_add_kernel(const float* __restrict__ Y, const int* __restrict__ top,
-                                   const int* __restrict__ mode_bath, const double* __restrict__ vdiag, int n_top,
-                                   int M, int logd, int herm, long long stride, double s_out, double alpha,
+// Closure term of a stage: out_{top i}(r, c) += alpha sum_k -i (v_j(r) - v_j(c))
+// coef[k][n_{i,k}](r, c) u_{top i}(r, c)   (the dropped up coupling, with the
+// up neighbour predicted elementwise).  Full or Hermitian-packed slabs.
+__global__ void closure_lin_kernel(const double2* __restrict__ u, const int* __restrict__ top,
+                                   const int8_t* __restrict__ top_occ, const int* __restrict__ mode_bath,
+                                   const double* __restrict__ vdiag, const double2* __restrict__ coef, int n_top,
+                                   int M, int maxd, int logd, int herm, long long stride, double alpha,
                                    double2* out)
 {
-    const int D = 1 << logd;
-    const int d2 = D * D;
+    const int D = 1 << logd, d2 = D * D;
+    const int nel = herm ? herm_elems(logd) : d2;
     const int i = blockIdx.y;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= d2 || i >= n_top) return;
-    const int r = e >> logd, c = e & (D - 1);
-    if (herm && r > c) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nel || i >= n_top) return;
+    int r, c;
+    if (herm) {
+        herm_coords(q, logd, r, c);
+    } else {
+        r = q >> logd;
+        c = q & (D - 1);
+    }
+    const int e = (r << logd) + c;
+    const double2 x = u[top[i] * stride + q];
     double sr = 0.0, si = 0.0;
     for (int k = 0; k < M; ++k) {
         const int j = mode_bath[k];
         const double del = vdiag[j * D + r] - vdiag[j * D + c];
         if (del == 0.0) continue;
-        const float* y = Y + (static_cast<long long>(i) * M + k) * 2 * d2;
-        const int et = (c << logd) + r;  // transposed element
-        sr += del * (0.5 * (static_cast<double>(y[2 * e]) + y[2 * et]));
-        si += del * (0.5 * (static_cast<double>(y[2 * e + 1]) - y[2 * et + 1]));
+        const double2 a = coef[(static_cast<long long>(k) * maxd + top_occ[i * M + k]) * d2 + e];
+        // -i del (a x)
+        sr += del * (a.x * x.y + a.y * x.x);
+        si -= del * (a.x * x.x - a.y * x.y);
     }
-    // -i del Y = del (Y.y - i Y.x)
-    double2* o = out + top[i] * stride + (herm ? herm_index(r, c, logd) : e);
-    o->x += alpha * s_out * si;
-    o->y -= alpha * s_out * sr;
+    double2* o = out + top[i] * stride + q;
+    o->x += alpha * sr;
+    o->y += alpha * si;
 }
 
 // sum of squares of FP32 complex data (deterministic two-level sum)
@@ -393,6 +462,7 @@ struct hx_mlp {
     float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
     bf16* wh = nullptr;
     long long adam_t = 0;
+    uint64_t version = 0;  // bumped whenever the parameters change
     // activations for one batch
     int cap = 0;
     bf16 *X = nullptr, *H1 = nullptr, *H2 = nullptr, *dYh = nullptr, *dZ2h = nullptr, *dZ1h = nullptr;
@@ -454,13 +524,10 @@ void mlp_forward(hx_mlp* n, int B, cudaStream_t s)
                                 GemmOut{n->w + n->ob3, n->Y, nullptr, nullptr, n->out_dim}, s);
 }
 
-// MSE loss against n->T and the gradient of every parameter into n->g; returns the loss.
-int mlp_backward(hx_mlp* n, int B, float* loss, cudaStream_t s)
+// Gradient of every parameter into n->g from dL/dY already in n->dYf / n->dYh.
+void mlp_backward_dy(hx_mlp* n, int B, cudaStream_t s)
 {
     using namespace hx;
-    const long long ny = static_cast<long long>(B) * n->out_dim;
-    const int nb = 148;
-    mse_kernel<<<nb, 256, 0, s>>>(n->Y, n->T, ny, 2.0f / static_cast<float>(ny), n->dYf, n->dYh, n->partial);
     const bf16* W = n->wh;
     // layer 3
     gemm<true, false, kEpiStore>(n->out_dim, n->hidden, B, n->dYh, n->out_dim, n->H2, n->hidden,
@@ -478,19 +545,32 @@ int mlp_backward(hx_mlp* n, int B, float* loss, cudaStream_t s)
     gemm<true, false, kEpiStore>(n->hidden, n->in_dim, B, n->dZ1h, n->hidden, n->X, n->in_ld,
                                  GemmOut{nullptr, n->g + n->oW1, nullptr, nullptr, n->in_dim}, s);
     colsum_kernel<<<(n->hidden + 255) / 256, 256, 0, s>>>(n->dZ1f, B, n->hidden, n->hidden, n->g + n->ob1);
-    if (loss) {
-        HX_CUDA_TRY(cudaMemcpyAsync(n->pinned, n->partial, nb * sizeof(float), cudaMemcpyDeviceToHost, s));
-        HX_CUDA_TRY(cudaStreamSynchronize(s));
-        double acc = 0.0;
-        for (int i = 0; i < nb; ++i) acc += n->pinned[i];
-        *loss = static_cast<float>(acc / static_cast<double>(ny));
-    }
+}
+
+// Sum of the per-block loss partials (148 blocks) divided by count.
+int mlp_loss_of_partials(hx_mlp* n, double count, float* loss, cudaStream_t s)
+{
+    HX_CUDA_TRY(cudaMemcpyAsync(n->pinned, n->partial, 148 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HX_CUDA_TRY(cudaStreamSynchronize(s));
+    double acc = 0.0;
+    for (int i = 0; i < 148; ++i) acc += n->pinned[i];
+    *loss = static_cast<float>(acc / count);
     return HX_OK;
+}
+
+// MSE loss against n->T and the gradient of every parameter into n->g; returns the loss.
+int mlp_backward(hx_mlp* n, int B, float* loss, cudaStream_t s)
+{
+    const long long ny = static_cast<long long>(B) * n->out_dim;
+    hx::mse_kernel<<<148, 256, 0, s>>>(n->Y, n->T, ny, 2.0f / static_cast<float>(ny), n->dYf, n->dYh, n->partial);
+    mlp_backward_dy(n, B, s);
+    return loss ? mlp_loss_of_partials(n, static_cast<double>(ny), loss, s) : HX_OK;
 }
 
 void mlp_adam(hx_mlp* n, float lr, cudaStream_t s)
 {
     n->adam_t += 1;
+    n->version += 1;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - std::pow(b1, static_cast<float>(n->adam_t));
     const float c2 = 1.f - std::pow(b2, static_cast<float>(n->adam_t));
@@ -516,19 +596,36 @@ void mlp_release(hx_mlp* n)
 // Closure object: index maps, device training set, the MLP
 // ---------------------------------------------------------------------------
 
+// The closure predicts the dropped up neighbour of a top-tier ADO n
+// elementwise: rho_{n+e_k}(r, c) ~ A(k, n_k, r, c) rho_n(r, c), the complex
+// coefficient A coming from the MLP on the features of (k, n_k, r, c)
+// (closure_features).  The equations are linear, and so is this prediction
+// in rho_n.  After training, A is evaluated once for every (k, n_k, r, c) into
+// a coefficient table, so a stage costs one elementwise kernel.
 struct hx_closure {
     hx_mlp* net = nullptr;
     int d = 0, logd = 0, d2 = 0, M = 0, J = 0;
     uint32_t coarse_depth = 0, fine_depth = 0;
+    int maxd = 0;                // n_k of a top-tier ADO is in [0, maxd)
     int n_top = 0, n_up = 0;
     std::vector<int> mode_bath;
     int* top_coarse = nullptr;   // [n_top] coarse index of each top-tier ADO
     int* top_fine = nullptr;     // [n_top] its index in the fine hierarchy
+    int8_t* top_occ = nullptr;   // [n_top][M] occupation n_k of each top-tier ADO
     int* up_fine = nullptr;      // [n_up] fine index of each distinct up neighbour
     int* up_local = nullptr;     // [n_top][M] which of them is n_top[i] + e_k
     int* mode_bath_d = nullptr;  // [M]
+    double* vdiag = nullptr;     // [J][d] coupling diagonals
+    double* hdiag = nullptr;     // [d] diagonal of H
+    double inv_e = 1.0;          // 1 / (max E - min E)
     float2* din = nullptr;       // [cap][n_top][d2]
     float2* dout = nullptr;      // [cap][n_up][d2]
+    float2* xin = nullptr;       // [batch] training inputs (scaled elements)
+    float2* tgt = nullptr;       // [batch] training targets
+    int sample_cap = 0;
+    float2* raw = nullptr;       // [M][maxd][d2] network output A
+    double2* coef = nullptr;     // [M][maxd][d2] Hermitian part of A times s_out / s_in
+    uint64_t table_version = ~0ull;  // network version the table was built from
     int cap = 0, n_snap = 0;
     double s_in = 1.0, s_out = 1.0;  // RMS scales of inputs and targets
     bool scaled = false;
@@ -541,7 +638,8 @@ void closure_release(hx_closure* c)
 {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* p[] = {c->top_coarse, c->top_fine, c->up_fine, c->up_local, c->mode_bath_d, c->din, c->dout};
+    void* p[] = {c->top_coarse, c->top_fine, c->up_fine, c->up_local, c->mode_bath_d, c->din, c->dout,
+                 c->top_occ, c->vdiag, c->hdiag, c->xin, c->tgt, c->raw, c->coef};
     for (void* q : p)
         if (q) cudaFree(q);
     if (c->net) mlp_release(c->net);
@@ -573,25 +671,51 @@ bool hx::closure_matches_hierarchy(const hx_closure* cl, int d, int M, long long
     return cl->d == d && cl->M == M && static_cast<long long>(Hc) == H;
 }
 
+namespace {
+
+// Evaluate the network on every (k, n_k, r, c) and store the Hermitian part
+// of A, times s_out / s_in, in the coefficient table.
+int build_table(hx_closure* cl, cudaStream_t s)
+{
+    hx_mlp* n = cl->net;
+    const long long rows = static_cast<long long>(cl->M) * cl->maxd * cl->d2;
+    const int chunk = 8192;
+    int rc = mlp_reserve(n, chunk);
+    if (rc != HX_OK) return rc;
+    for (long long r0 = 0; r0 < rows; r0 += chunk) {
+        const int cnt = static_cast<int>(std::min<long long>(chunk, rows - r0));
+        hx::table_features_kernel<<<(cnt + 127) / 128, 128, 0, s>>>(cl->mode_bath_d, cl->vdiag, cl->hdiag, cl->inv_e,
+                                                                   cl->M, cl->maxd, cl->logd, n->in_ld, r0, cnt, n->X);
+        mlp_forward(n, cnt, s);
+        HX_CUDA_TRY(cudaMemcpyAsync(cl->raw + r0, n->Y, cnt * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+    }
+    hx::table_kernel<<<static_cast<unsigned>((rows + 255) / 256), 256, 0, s>>>(cl->raw, rows, cl->logd,
+                                                                               cl->s_out / cl->s_in, cl->coef);
+    HX_CUDA_TRY(cudaGetLastError());
+    cl->table_version = n->version;
+    return HX_OK;
+}
+
+}  // namespace
+
 namespace hx {
 int closure_stage(hx_closure* cl, const ::hx_ctx* c, const double2* u, double2* out, double alpha, cudaStream_t s)
 {
     if (!cl || !cl->scaled) return HX_OK;
-    const int rows = cl->n_top * cl->M;
-    hx_mlp* n = cl->net;
-    int rc = mlp_reserve(n, rows);
-    if (rc != HX_OK) return rc;
+    if (cl->table_version != cl->net->version) {
+        const int rc = build_table(cl, s);
+        if (rc != HX_OK) return rc;
+    }
     const int herm = c->herm ? 1 : 0;
     const long long stride = static_cast<long long>(c->slab_store);
-    closure_input_kernel<<<rows, 256, 0, s>>>(u, cl->top_coarse, cl->n_top, cl->M, cl->d2, cl->logd, herm, stride,
-                                              static_cast<float>(1.0 / cl->s_in), n->in_ld, n->X);
-    mlp_forward(n, rows, s);
-    dim3 grid((cl->d2 + 255) / 256, cl->n_top);
-    closure_add_kernel<<<grid, 256, 0, s>>>(n->Y, cl->top_coarse, cl->mode_bath_d, c->vdiag, cl->n_top, cl->M,
-                                           cl->logd, herm, stride, cl->s_out, alpha, out);
+    const int nel = herm ? herm_elems(cl->logd) : cl->d2;
+    dim3 grid((nel + 255) / 256, cl->n_top);
+    closure_lin_kernel<<<grid, 256, 0, s>>>(u, cl->top_coarse, cl->top_occ, cl->mode_bath_d, cl->vdiag, cl->coef,
+                                           cl->n_top, cl->M, cl->maxd, cl->logd, herm, stride, alpha, out);
     return HX_OK;
 }
 }  // namespace hx
+
 
 extern "C" {
 
@@ -674,6 +798,7 @@ int hx_mlp_set_params(hx_mlp* n, const float* params, uint64_t count)
     HX_CUDA_TRY(cudaGetLastError());
     HX_CUDA_TRY(cudaStreamSynchronize(n->stream));
     n->adam_t = 0;
+    n->version += 1;
     return HX_OK;
 }
 
@@ -774,7 +899,8 @@ int hx_closure_create(const hx_problem* coarse, uint32_t fine_max_depth, uint32_
 {
     if (!out) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL closure output");
     *out = nullptr;
-    if (!coarse || !coarse->baths || coarse->n_baths == 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL problem");
+    if (!coarse || !coarse->baths || coarse->n_baths == 0 || !coarse->h_diag)
+        return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL problem");
     const uint32_t d = coarse->dim;
     if (d < 2 || d > 64 || (d & (d - 1)) != 0) return fail(HX_ERR_INVALID_DIMENSION, "closures need 2 <= dim <= 64");
     if (coarse->max_depth < 2 || fine_max_depth <= coarse->max_depth)
@@ -810,9 +936,24 @@ int hx_closure_create(const hx_problem* coarse, uint32_t fine_max_depth, uint32_
     c->J = static_cast<int>(coarse->n_baths);
     c->coarse_depth = coarse->max_depth;
     c->fine_depth = fine_max_depth;
+    c->maxd = static_cast<int>(coarse->max_depth);
     c->mode_bath = mb;
+    // operators for the features: coupling diagonals and the diagonal of H
+    std::vector<double> vd(static_cast<size_t>(c->J) * d), hd(coarse->h_diag, coarse->h_diag + d);
+    for (int j = 0; j < c->J; ++j) {
+        if (!coarse->baths[j].coupling_diag) return bail(fail(HX_ERR_UNSUPPORTED_BATH, "coupling operator is NULL"));
+        if (coarse->baths[j].coupling_flip)
+            for (int b = 0; (1u << b) < d; ++b)
+                if (coarse->baths[j].coupling_flip[b] != 0.0)
+                    return bail(fail(HX_ERR_UNSUPPORTED_EXECUTION, "closures need diagonal coupling operators"));
+        std::copy(coarse->baths[j].coupling_diag, coarse->baths[j].coupling_diag + d,
+                  vd.begin() + static_cast<size_t>(j) * d);
+    }
+    const double emax = *std::max_element(hd.begin(), hd.end()), emin = *std::min_element(hd.begin(), hd.end());
+    c->inv_e = emax > emin ? 1.0 / (emax - emin) : 1.0;
     // top tier of the coarse hierarchy and the fine indices of its up neighbours
     std::vector<int> top_c, top_f, up_f, up_loc;
+    std::vector<int8_t> occ;
     std::map<int, int> up_index;
     for (uint64_t i = 0; i < Hc; ++i) {
         std::vector<int32_t> v(rc_rows.begin() + i * M, rc_rows.begin() + (i + 1) * M);
@@ -821,6 +962,7 @@ int hx_closure_create(const hx_problem* coarse, uint32_t fine_max_depth, uint32_
         if (tier != static_cast<int>(coarse->max_depth) - 1) continue;
         top_c.push_back(static_cast<int>(i));
         top_f.push_back(fine_of.at(v));
+        for (int k = 0; k < M; ++k) occ.push_back(static_cast<int8_t>(v[k]));
         for (int k = 0; k < M; ++k) {
             std::vector<int32_t> w = v;
             w[k] += 1;
@@ -844,6 +986,17 @@ int hx_closure_create(const hx_problem* coarse, uint32_t fine_max_depth, uint32_
     if (e == cudaSuccess) e = dalloc(&c->mode_bath_d, mb.size());
     if (e == cudaSuccess) e = dalloc(&c->din, static_cast<size_t>(capacity) * c->n_top * c->d2);
     if (e == cudaSuccess) e = dalloc(&c->dout, static_cast<size_t>(capacity) * c->n_up * c->d2);
+    const size_t table = static_cast<size_t>(M) * c->maxd * c->d2;
+    if (e == cudaSuccess) e = dalloc(&c->top_occ, occ.size());
+    if (e == cudaSuccess) e = dalloc(&c->vdiag, vd.size());
+    if (e == cudaSuccess) e = dalloc(&c->hdiag, hd.size());
+    if (e == cudaSuccess) e = dalloc(&c->raw, table);
+    if (e == cudaSuccess) e = dalloc(&c->coef, table);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->top_occ, occ.data(), occ.size(), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->vdiag, vd.data(), vd.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->hdiag, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->top_coarse, top_c.data(), top_c.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->top_fine, top_f.data(), top_f.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->up_fine, up_f.data(), up_f.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
@@ -852,7 +1005,8 @@ int hx_closure_create(const hx_problem* coarse, uint32_t fine_max_depth, uint32_
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return bail(hx::cuda_fail(e, "closure set-up"));
     c->cap = static_cast<int>(capacity);
-    if ((rc = hx_mlp_create(2 * c->d2 + M, hidden, 2 * c->d2, seed, &c->net)) != HX_OK) return bail(rc);
+    if ((rc = hx_mlp_create(static_cast<uint32_t>(M + 3 + c->maxd), hidden, 2, seed, &c->net)) != HX_OK)
+        return bail(rc);
     *out = c;
     return HX_OK;
 }
@@ -923,15 +1077,27 @@ int hx_closure_train(hx_closure* c, uint32_t iters, uint32_t batch, float lr, ui
     }
     int rc = mlp_reserve(n, static_cast<int>(batch));
     if (rc != HX_OK) return rc;
+    if (c->sample_cap < static_cast<int>(batch)) {
+        cudaFree(c->xin);
+        cudaFree(c->tgt);
+        c->xin = c->tgt = nullptr;
+        c->sample_cap = 0;
+        HX_CUDA_TRY(cudaMalloc(&c->xin, batch * sizeof(float2)));
+        HX_CUDA_TRY(cudaMalloc(&c->tgt, batch * sizeof(float2)));
+        c->sample_cap = static_cast<int>(batch);
+    }
     // cosine learning-rate decay over the call
     for (uint32_t it = 0; it < iters && rc == HX_OK; ++it) {
-        hx::gather_closure_kernel<<<batch, 256, 0, n->stream>>>(
-            c->din, c->dout, c->up_local, c->n_snap, c->n_top, c->n_up, c->M, c->d2,
-            static_cast<float>(1.0 / c->s_in), static_cast<float>(1.0 / c->s_out), n->in_ld, static_cast<int>(batch),
-            seed + it, n->X, n->T);
+        hx::gather_closure_kernel<<<(batch + 127) / 128, 128, 0, n->stream>>>(
+            c->din, c->dout, c->up_local, c->top_occ, c->mode_bath_d, c->vdiag, c->hdiag, c->inv_e, c->n_snap,
+            c->n_top, c->n_up, c->M, c->maxd, c->logd, static_cast<float>(1.0 / c->s_in),
+            static_cast<float>(1.0 / c->s_out), n->in_ld, static_cast<int>(batch), seed + it, n->X, c->xin, c->tgt);
         mlp_forward(n, static_cast<int>(batch), n->stream);
+        hx::closure_loss_kernel<<<148, 256, 0, n->stream>>>(n->Y, c->xin, c->tgt, static_cast<int>(batch), n->dYf,
+                                                            n->dYh, n->partial);
+        mlp_backward_dy(n, static_cast<int>(batch), n->stream);
         float l = 0.f;
-        rc = mlp_backward(n, static_cast<int>(batch), loss_trace ? &l : nullptr, n->stream);
+        if (loss_trace) rc = mlp_loss_of_partials(n, static_cast<double>(batch), &l, n->stream);
         if (loss_trace) loss_trace[it] = l;
         const float f = 0.5f * (1.f + std::cos(3.14159265358979f * static_cast<float>(it) / static_cast<float>(iters)));
         mlp_adam(n, lr * (0.05f + 0.95f * f), n->stream);
@@ -939,6 +1105,7 @@ int hx_closure_train(hx_closure* c, uint32_t iters, uint32_t batch, float lr, ui
         if (e != cudaSuccess) rc = hx::cuda_fail(e, "closure training");
     }
     if (rc != HX_OK) return rc;
+    if ((rc = build_table(c, n->stream)) != HX_OK) return rc;
     HX_CUDA_TRY(cudaStreamSynchronize(n->stream));
     return HX_OK;
 }
@@ -950,6 +1117,7 @@ int hx_closure_set_scales(hx_closure* c, double s_in, double s_out)
     c->s_in = s_in;
     c->s_out = s_out;
     c->scaled = true;
+    c->table_version = ~0ull;  // rebuilt with the new scales before the next stage
     return HX_OK;
 }
 

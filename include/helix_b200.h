@@ -275,9 +275,14 @@ int hx_batch_read_rho0(hx_batch* batch, uint32_t instance, double* out, uint64_t
  * Param::JMax and drops the next tier (src/parameters.cu:31,
  * src/initialize_detail.h:196-213); a closure supplies, for every ADO n of the
  * top tier and every mode k, a prediction of the dropped up neighbour
- * rho_{n+e_k} from rho_n, by a small MLP (BF16 weights, FP32 accumulation)
- * trained on the device from deeper (fine) hierarchies.  No counterpart in the
- * reference.
+ * rho_{n+e_k}, elementwise and linear in rho_n:
+ *   rho_{n+e_k}(r, c) ~ A(k, n_k, r, c) rho_n(r, c),
+ * the complex coefficient A given by a small MLP (BF16 weights, FP32
+ * accumulation) from the features of (k, n_k, r, c): one-hot k, the coupling
+ * diagonal of k's bath at r and at c, (E_r - E_c) scaled by the spread of the
+ * diagonal of H, one-hot n_k.  The network is trained on the device from
+ * deeper (fine) hierarchies; its Hermitian part, evaluated once into a table,
+ * is what the stages apply.  No counterpart in the reference.
  * ------------------------------------------------------------------------ */
 typedef struct hx_mlp hx_mlp;
 
@@ -304,9 +309,11 @@ int hx_mlp_train(hx_mlp* mlp, const float* x, const float* t, uint32_t rows, uin
 typedef struct hx_closure hx_closure;
 
 /* Closure for the truncated (coarse) problem `coarse` (2 <= dim <= 64,
- * max_depth >= 2), trained from fine hierarchies of the same system with
- * max_depth = fine_max_depth; the training set holds up to `capacity`
- * snapshots on the device; MLP width `hidden`. */
+ * max_depth >= 2, diagonal coupling operators), trained from fine hierarchies
+ * of the same system with max_depth = fine_max_depth; the training set holds
+ * up to `capacity` snapshots on the device.  The MLP maps modes + 3 +
+ * max_depth features through two GELU layers of width `hidden` to the two
+ * reals of A. */
 int hx_closure_create(const hx_problem* coarse, uint32_t fine_max_depth, uint32_t hidden, uint32_t capacity,
                       uint64_t seed, hx_closure** out);
 void hx_closure_destroy(hx_closure* closure);
@@ -316,8 +323,10 @@ int hx_closure_info(const hx_closure* closure, uint32_t* top_ados, uint32_t* up_
 /* Add one snapshot from the current state of a fine-hierarchy context: the
  * coarse top-tier ADOs and their up neighbours. */
 int hx_closure_harvest(hx_closure* closure, hx_ctx* fine);
-/* Train on the snapshots (input and target scaled by their RMS over the set,
- * fixed at the first call after a harvest; cosine-decayed Adam). */
+/* Train on the snapshots: minibatches of `batch` elements (snapshot, top-tier
+ * ADO, mode, element with a nonzero commutator weight), loss mean |A x - t|^2
+ * with x, t scaled by their RMS over the set (fixed at the first call),
+ * cosine-decayed Adam; then rebuild the coefficient table. */
 int hx_closure_train(hx_closure* closure, uint32_t iters, uint32_t batch, float lr, uint64_t seed,
                      float* loss_trace);
 /* Scales of a closure whose parameters were set from elsewhere. */

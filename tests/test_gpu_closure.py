@@ -2,7 +2,8 @@
 gradients against the FP64 restatement with the same BF16 rounding points
 (oracle/mlp_oracle.py), training convergence, and the closure itself: a
 truncated hierarchy plus the trained network tracks the deep hierarchy's
-rho_0(t) better than the truncated hierarchy alone, on held-out seeds."""
+rho_0(t) better than the truncated hierarchy alone, on held-out seeds, and
+its coefficient table is the network's output on the documented features."""
 import numpy as np
 import pytest
 
@@ -74,7 +75,7 @@ def test_closure_beats_truncation_on_held_out_seeds():
     coarse_depth, fine_depth = 2, 5
     train_seeds, test_seeds = [100 + s for s in range(6)], [900, 901]
     coarse0 = S.spin_glass(n, seed=train_seeds[0], depth=coarse_depth, K=K, h=1.0, dt=0.01)
-    cl = capi.Closure(coarse0, fine_max_depth=fine_depth + 1, hidden=512, capacity=len(train_seeds) * steps // every)
+    cl = capi.Closure(coarse0, fine_max_depth=fine_depth + 1, hidden=64, capacity=len(train_seeds) * steps // every)
     for s in train_seeds:
         fine = S.spin_glass(n, seed=s, depth=fine_depth, K=K, h=1.0, dt=0.01)
         with capi.Context(fine) as ctx:
@@ -84,8 +85,9 @@ def test_closure_beats_truncation_on_held_out_seeds():
     info = cl.info()
     assert info["snapshots"] == len(train_seeds) * steps // every
     assert info["top_ados"] == 45 and info["up_ados"] > 0
-    trace = cl.train(iters=4000, batch=512, lr=1e-3, seed=4)
-    assert np.all(np.isfinite(trace)) and trace[-100:].mean() < 0.1 * trace[:20].mean()
+    trace = cl.train(iters=1500, batch=4096, lr=3e-3, seed=4)
+    # an elementwise linear model keeps a loss floor well above zero; it must drop clearly
+    assert np.all(np.isfinite(trace)) and trace[-100:].mean() < 0.8 * trace[:20].mean()
     gains = []
     for s in test_seeds:
         fine = S.spin_glass(n, seed=s, depth=fine_depth, K=K, h=1.0, dt=0.01)
@@ -96,9 +98,11 @@ def test_closure_beats_truncation_on_held_out_seeds():
         e_plain = max(_trace_distance(plain[t], ref[t]) for t in range(0, steps, 20))
         e_closed = max(_trace_distance(closed[t], ref[t]) for t in range(0, steps, 20))
         gains.append(e_plain / e_closed)
-    # truncation at L=2 leaves a trace distance of ~2e-2 against L=5 here; the
-    # trained closure must cut it by a factor of 1.5 or more
-    assert min(gains) > 1.5, gains
+    # truncation at L=2 leaves a trace distance of ~2e-2 against L=5 here; an
+    # elementwise linear closure fitted by least squares per (mode, bit class,
+    # n_k) cuts it ~3.8x, the trained network (which also sees E_r - E_c) ~4.1x;
+    # it must cut it by a factor of 3 or more
+    assert min(gains) > 3.0, gains
     cl.close()
 
 
@@ -136,3 +140,58 @@ def test_closure_on_packed_and_full_slabs_agree():
     assert np.max(np.abs(trajs[0] - plain)) > 1e-8  # the closure term is there
     for cl in made:
         cl.close()
+
+
+def test_closure_term_is_the_network_on_the_documented_features():
+    """The closure term a stage adds equals, element by element,
+    sum_k -i (v_j(r) - v_j(c)) A_h(k, n_k, r, c) rho_n(r, c) (s_out / s_in)
+    for every top-tier ADO n, with A from the network on the features
+    [one-hot k, v_j(r), v_j(c), (E_r - E_c) / (max E - min E), one-hot n_k]
+    and A_h = (A(r, c) + conj A(c, r)) / 2 (its Hermitian part)."""
+    n, K = 3, 1
+    coarse = S.spin_glass(n, seed=77, depth=2, K=K, h=0.8, dt=0.01)
+    fine = S.spin_glass(n, seed=77, depth=3, K=K, h=0.8, dt=0.01)
+    cl = capi.Closure(coarse, fine_max_depth=4, hidden=32, capacity=3, seed=2)
+    with capi.Context(fine) as ctx:
+        for _ in range(3):
+            ctx.step(20)
+            cl.harvest(ctx)
+    cl.train(iters=30, batch=256, lr=1e-3, seed=1)
+    info = cl.info()
+    d, M, maxd = coarse.dim, coarse.modes, coarse.max_depth
+    rows, _ = capi.hierarchy_tables(M, maxd)
+    top = [i for i in range(rows.shape[0]) if rows[i].sum() == maxd - 1]
+    E = np.asarray(coarse.h_diag)
+    inv_e = 1.0 / (E.max() - E.min())
+    feats = []
+    for k in range(M):
+        v = np.asarray(coarse.baths[k // (K + 1)].v_diag)
+        for nk in range(maxd):
+            for r in range(d):
+                for c in range(d):
+                    f = np.zeros(M + 3 + maxd, np.float32)
+                    f[k] = 1.0
+                    f[M], f[M + 1] = v[r], v[c]
+                    f[M + 2] = np.float32((E[r] - E[c]) * inv_e)
+                    f[M + 3 + nk] = 1.0
+                    feats.append(f)
+    A = cl.mlp.forward(np.array(feats)).astype(np.float64)
+    A = (A[:, 0] + 1j * A[:, 1]).reshape(M, maxd, d, d)
+    Ah = 0.5 * (A + np.conj(np.transpose(A, (0, 1, 3, 2)))) * (info["s_out"] / info["s_in"])
+    rng = np.random.default_rng(3)
+    with capi.Context(coarse) as plain, capi.Context(coarse) as closed:
+        x = rng.standard_normal((plain.size, d, d)) + 1j * rng.standard_normal((plain.size, d, d))
+        x = 0.5 * (x + np.conj(np.transpose(x, (0, 2, 1))))
+        plain.set_state(x)
+        closed.set_state(x)
+        cl.attach(closed)
+        diff = closed.rhs() - plain.rhs()
+    want = np.zeros_like(diff)
+    for i in top:
+        for k in range(M):
+            v = np.asarray(coarse.baths[k // (K + 1)].v_diag)
+            delta = v[:, None] - v[None, :]
+            want[i] += -1j * delta * Ah[k, rows[i][k]] * x[i]
+    assert np.max(np.abs(want)) > 0
+    assert np.max(np.abs(diff - want)) <= 1e-10 * max(1.0, np.max(np.abs(want)))
+    cl.close()
