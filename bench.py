@@ -68,6 +68,10 @@ def load_peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
+def info_kernels_per_stage(ctx) -> int:
+    return int(ctx.info.kernels_per_step) // 4
+
+
 def profiled_traffic(config: str, kernel: str = "fused_kernel") -> float | None:
     """DRAM bytes per launch of `kernel` from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_{config}_ncu.txt")
@@ -272,7 +276,11 @@ def run_ours(args, cfg: dict) -> None:
     peak, peak_kind = load_peaks()
     packed = bool(ctx.hermitian_packed)
     kernel = "herm_kernel" if packed else "fused_kernel"
+    # DRAM bytes of one stage: the stage kernel plus the up-term kernel (committed ncu summaries)
     traffic = profiled_traffic(args.config, kernel)
+    up_traffic = profiled_traffic(args.config, "upterm_kernel")
+    if traffic is not None and up_traffic is not None and info_kernels_per_stage(ctx) == 2:
+        traffic += up_traffic
     slab_elems = p.dim * (p.dim + 1) // 2 if packed else p.dim * p.dim
 
     # ---- end to end through the C ABI with host buffers (e2e) --------------
@@ -321,6 +329,8 @@ def run_ours(args, cfg: dict) -> None:
                          "algorithmic_bytes_per_launch": per_launch_bytes,
                          "kernel": (f"{kernel}<{p.dim.bit_length() - 1}> + upterm_kernel per stage"
                                     + (" (Hermitian-packed slabs)" if packed else "")),
+                         "traffic_source": f"dram bytes of one stage from profiles/{kernel}_{args.config}_ncu.txt "
+                                           f"+ profiles/upterm_kernel_{args.config}_ncu.txt",
                          "launch_ms": launch_ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": slab_elems * 16 + 24,
