@@ -91,6 +91,31 @@ def test_rhs_general_diagonal_coupling():
     o.close()
 
 
+@pytest.mark.parametrize("n", [5, 6])
+def test_packed_path_general_diagonal_coupling(n):
+    """d = 32, 64 with non-Pauli diagonal couplings: the packed fused kernel's
+    table-driven branch (both commutator and anti-commutator weights active)."""
+    p = S.spin_glass(n, seed=40 + n, depth=2, K=1, h=0.6, dt=0.005)
+    rng = np.random.default_rng(n)
+    for b in p.baths:
+        b.v_diag = rng.standard_normal(p.dim)
+    o = O.Oracle(p)
+    with capi.Context(p) as ctx:
+        assert ctx.hermitian_packed
+        x = _random_state(ctx.size, p.dim, 13, hermitian=True) * 1e-2
+        x[0] = S.initial_rho0(p.dim)
+        ctx.set_state(x)
+        got = ctx.rhs()
+        want = o.rhs(x)
+        assert np.max(np.abs(got - want)) <= 1e-12 * max(1.0, np.max(np.abs(want)))
+        o.set_state(x)
+        ctx.step(3)
+        ctx.sync()
+        o.run(3)
+        assert np.max(np.abs(ctx.state() - o.state())) <= TOL
+    o.close()
+
+
 def test_c1_spin_glass_full_trajectory():
     """The d=16, 12-mode, L=3 (455 ADO) spin glass: 1000 steps of rho_0(t), <H>(t)."""
     p = S.spin_glass(4, seed=2024, depth=3, K=2, h=1.0, dt=0.01)
