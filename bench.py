@@ -140,19 +140,39 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(cfg: dict, steps: int) -> dict:
-    """Time the FP64 CPU oracle (the reference has no CPU path) on host cores."""
+    """Time the FP64 CPU oracle (the reference has no CPU path) on all host
+    threads, then one full step on one thread."""
     from oracle import oracle as O
     p = make_problem(cfg)
     o = O.Oracle(p)
+    cores = O.threads()
     o.run(1)  # warm
     t0 = time.perf_counter()
     o.run(steps)
     dt = time.perf_counter() - t0
     size = o.size
+    O.set_threads(1)
+    t0 = time.perf_counter()
+    o.run(1)
+    dt1 = time.perf_counter() - t0
+    O.set_threads(cores)
     o.close()
-    return {"value": size * steps / dt, "unit": UNIT, "cores": O.threads(), "kind": "port",
-            "sample": f"{steps} full steps of the {size}-ADO hierarchy ({cfg['workload']}), FP64 oracle, OpenMP"}
+    return {"value": size * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} full steps of the {size}-ADO hierarchy ({cfg['workload']}), FP64 oracle, OpenMP",
+            "one_core": {"value": size / dt1, "unit": UNIT, "sample": "1 full step on 1 thread"},
+            "nproc": os.cpu_count(), "cpu_model": cpu_model()}
 
 
 def run_reference(args, cfg: dict) -> None:

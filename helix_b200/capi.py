@@ -34,6 +34,7 @@ EXPORTS = [
     "hx_ctx_info", "hx_ctx_counters", "hx_ctx_step", "hx_ctx_step_trace", "hx_ctx_sync",
     "hx_ctx_read_rho0", "hx_ctx_observables", "hx_ctx_read_state", "hx_ctx_write_state",
     "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_check_finite", "hx_rhs_noalloc",
+    "hx_ctx_save_snapshot", "hx_ctx_load_snapshot", "hx_write_energy_trace",
     "hx_batch_create", "hx_batch_destroy", "hx_batch_set_stream", "hx_batch_info", "hx_batch_tune",
     "hx_batch_step", "hx_batch_sync", "hx_batch_read_rho0",
     "hx_mlp_create", "hx_mlp_destroy", "hx_mlp_num_params", "hx_mlp_get_params", "hx_mlp_set_params",
@@ -130,6 +131,9 @@ def lib():
             L.hx_ctx_rhs.argtypes = [vp, vp, u64]
             L.hx_ctx_check_finite.argtypes = [vp]
             L.hx_rhs_noalloc.argtypes = [C.POINTER(_Problem), vp, vp, vp]
+            L.hx_ctx_save_snapshot.argtypes = [vp, C.c_char_p, C.c_uint32]
+            L.hx_ctx_load_snapshot.argtypes = [vp, C.c_char_p, C.c_uint32]
+            L.hx_write_energy_trace.argtypes = [C.c_char_p, vp, vp, C.c_uint64]
             L.hx_batch_create.argtypes = [C.POINTER(_Problem), u32, C.POINTER(BatchOptions), C.POINTER(vp)]
             L.hx_batch_destroy.argtypes = [vp]
             L.hx_batch_destroy.restype = None
@@ -256,6 +260,16 @@ def _problem_struct(problem, order: int = 4, dt: float | None = None, precision:
     return prob, keep
 
 
+def write_energy_trace(path: str, times, energies) -> None:
+    """times / energies as lines "time energy" (8 significant digits), the
+    reference CLI's outputEnergy.txt format."""
+    t = np.ascontiguousarray(times, np.float64)
+    e = np.ascontiguousarray(energies, np.float64)
+    if t.shape != e.shape or t.ndim != 1:
+        raise HxError(6, "times and energies must be 1-D arrays of equal length")
+    _check(lib().hx_write_energy_trace(os.fsencode(path), _p(t), _p(e), t.size))
+
+
 def rhs_noalloc(problem, rho_device_ptr: int, drho_device_ptr: int, stream_ptr: int | None = None) -> None:
     """drho = L(rho) through hx_rhs_noalloc (device pointers; allocates nothing)."""
     prob, keep = _problem_struct(problem)
@@ -376,6 +390,13 @@ class Context:
         out = np.zeros((self.size, self.dim, self.dim), np.complex128)
         _check(lib().hx_ctx_rhs(self._h, _p(out), 2 * out.size))
         return out
+
+    def save_snapshot(self, path: str, real_bytes: int = 4) -> None:
+        """The state in the reference's snapshot_rho<N>.dat format (float by default)."""
+        _check(lib().hx_ctx_save_snapshot(self._h, os.fsencode(path), real_bytes))
+
+    def load_snapshot(self, path: str, real_bytes: int = 4) -> None:
+        _check(lib().hx_ctx_load_snapshot(self._h, os.fsencode(path), real_bytes))
 
     def check_finite(self) -> None:
         _check(lib().hx_ctx_check_finite(self._h))

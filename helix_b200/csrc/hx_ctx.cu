@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
@@ -327,14 +328,15 @@ int read_error_flag(hx_ctx* c)
 }
 
 // Packed slab from a full row-major complex matrix (2 d^2 doubles); false
-// when the matrix is not Hermitian to 1e-12 of its largest element.
-bool pack_herm_host(const double* in, int logd, double2* pk)
+// when X - X^H exceeds rel_tol times the largest element.  Stores the upper
+// triangle, or with `average` the upper triangle of the Hermitian part.
+bool pack_herm_host(const double* in, int logd, double2* pk, double rel_tol = 1e-12, bool average = false)
 {
     const int D = 1 << logd, P = hx::herm_elems(logd);
     double scale2 = 0.0;
     for (size_t e = 0; e < static_cast<size_t>(D) * D; ++e)
         scale2 = std::max(scale2, in[2 * e] * in[2 * e] + in[2 * e + 1] * in[2 * e + 1]);
-    const double tol2 = 1e-24 * scale2;
+    const double tol2 = rel_tol * rel_tol * scale2;
     for (int i = 0; i < P; ++i) {
         int r, c;
         hx::herm_coords(i, logd, r, c);
@@ -343,7 +345,8 @@ bool pack_herm_host(const double* in, int logd, double2* pk)
             const double dr = in[2 * up] - in[2 * lo], di = in[2 * up + 1] + in[2 * lo + 1];
             if (dr * dr + di * di > tol2) return false;
         }
-        pk[i] = make_double2(in[2 * up], in[2 * up + 1]);
+        pk[i] = average ? make_double2(0.5 * (in[2 * up] + in[2 * lo]), 0.5 * (in[2 * up + 1] - in[2 * lo + 1]))
+                        : make_double2(in[2 * up], in[2 * up + 1]);
     }
     return true;
 }
@@ -926,6 +929,82 @@ int hx_ctx_write_state(hx_ctx* c, const double* in, uint64_t n)
     }
     HX_CUDA_TRY(cudaMemcpyAsync(c->rho, in, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
     c->counters.h2d_bytes += count * sizeof(double2);
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return HX_OK;
+}
+
+int hx_ctx_save_snapshot(hx_ctx* c, const char* path, uint32_t real_bytes)
+{
+    if (!c || !path) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    if (real_bytes != 4 && real_bytes != 8) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "real_bytes must be 4 or 8");
+    const size_t count = static_cast<size_t>(c->H) * c->slab;
+    std::vector<double> all(2 * count);
+    int rc = hx_ctx_read_state(c, all.data(), all.size());
+    if (rc != HX_OK) return rc;
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(HX_ERR_INVALID_RUNTIME_OPTION, std::string("cannot open ") + path + " for writing");
+    size_t wrote = 0;
+    if (real_bytes == 8) {
+        wrote = std::fwrite(all.data(), sizeof(double), all.size(), f);
+    } else {
+        std::vector<float> narrow(all.size());
+        for (size_t i = 0; i < all.size(); ++i) narrow[i] = static_cast<float>(all[i]);
+        wrote = std::fwrite(narrow.data(), sizeof(float), narrow.size(), f);
+    }
+    const bool closed = std::fclose(f) == 0;
+    if (wrote != all.size() || !closed) return fail(HX_ERR_INVALID_RUNTIME_OPTION, std::string("short write to ") + path);
+    return HX_OK;
+}
+
+int hx_ctx_load_snapshot(hx_ctx* c, const char* path, uint32_t real_bytes)
+{
+    if (!c || !path) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    if (real_bytes != 4 && real_bytes != 8) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "real_bytes must be 4 or 8");
+    const size_t count = static_cast<size_t>(c->H) * c->slab;
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(HX_ERR_INVALID_RUNTIME_OPTION, std::string("cannot open ") + path);
+    std::fseek(f, 0, SEEK_END);
+    const long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (size < 0 || static_cast<size_t>(size) != 2 * count * real_bytes) {
+        std::fclose(f);
+        return fail(HX_ERR_INVALID_RUNTIME_OPTION,
+                    std::string(path) + " holds " + std::to_string(size) + " bytes; this hierarchy needs " +
+                        std::to_string(2 * count * real_bytes));
+    }
+    std::vector<double> all(2 * count);
+    size_t got = 0;
+    if (real_bytes == 8) {
+        got = std::fread(all.data(), sizeof(double), all.size(), f);
+    } else {
+        std::vector<float> narrow(all.size());
+        got = std::fread(narrow.data(), sizeof(float), narrow.size(), f);
+        for (size_t i = 0; i < all.size(); ++i) all[i] = narrow[i];
+    }
+    std::fclose(f);
+    if (got != all.size()) return fail(HX_ERR_INVALID_RUNTIME_OPTION, std::string("short read from ") + path);
+    if (!c->herm) return hx_ctx_write_state(c, all.data(), all.size());
+    // Packed slabs hold the Hermitian part.  A snapshot written by another
+    // program (the reference computes (r, c) and (c, r) separately, in single
+    // precision by default) is Hermitian to its rounding only: accept up to
+    // 1e-5 of each ADO's largest element and store the Hermitian part.
+    const size_t n = static_cast<size_t>(c->H) * c->slab_store;
+    int rc = state_staging(c, n);
+    if (rc != HX_OK) return rc;
+    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    double2* pk = c->state_pinned;
+    std::vector<char> ok(static_cast<size_t>(c->H), 1);
+    parallel_for(c->H, [&](long long k) {
+        ok[k] = pack_herm_host(all.data() + 2 * static_cast<size_t>(k) * c->slab, c->logd, pk + k * c->slab_store,
+                               1e-5, true);
+    });
+    for (long long k = 0; k < c->H; ++k)
+        if (!ok[k])
+            return fail(HX_ERR_INVALID_RUNTIME_OPTION,
+                        "ADO " + std::to_string(k) + " of " + path +
+                            " is not Hermitian; load it into a context made with HX_FLAG_FULL_STATE");
+    HX_CUDA_TRY(cudaMemcpyAsync(c->rho, pk, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    c->counters.h2d_bytes += n * sizeof(double2);
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return HX_OK;
 }

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -213,6 +214,17 @@ int hx_seeded_couplings(uint32_t n, uint64_t seed, double* J)
             J[j * n + i] = z;
         }
     return HX_OK;
+}
+
+int hx_write_energy_trace(const char* path, const double* times, const double* energies, uint64_t n)
+{
+    if (!path || (n > 0 && (!times || !energies))) return hx::fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
+    std::FILE* f = std::fopen(path, "w");
+    if (!f) return hx::fail(HX_ERR_INVALID_RUNTIME_OPTION, std::string("cannot open ") + path + " for writing");
+    bool ok = true;
+    for (uint64_t i = 0; i < n && ok; ++i) ok = std::fprintf(f, "%.8g %.8g\n", times[i], energies[i]) > 0;
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? HX_OK : hx::fail(HX_ERR_INVALID_RUNTIME_OPTION, std::string("short write to ") + path);
 }
 
 }  // extern "C"

@@ -199,6 +199,24 @@ int hx_ctx_observables(hx_ctx* ctx, double* energy, double* trace_re, double* tr
 int hx_ctx_read_state(hx_ctx* ctx, double* out, uint64_t n);
 int hx_ctx_write_state(hx_ctx* ctx, const double* in, uint64_t n);
 
+/* Whole state to / from a file in the reference's snapshot format
+ * (snapshot_rho<N>.dat, src/cli_compatibility.cu:130-145, loader
+ * src/initialize.cu:266-285): hierarchy_size * d * d complex values in ADO
+ * order, row-major slabs, each value as its real then its imaginary part, in
+ * float (real_bytes = 4, the reference's default compiled precision) or
+ * double (8), native byte order, no header.  Loading checks the file size.
+ * On a context with Hermitian-packed slabs loading keeps the Hermitian part of
+ * each ADO and rejects an ADO whose anti-Hermitian part exceeds 1e-5 of its
+ * largest element (single-precision snapshots of another program are
+ * Hermitian to their rounding only). */
+int hx_ctx_save_snapshot(hx_ctx* ctx, const char* path, uint32_t real_bytes);
+int hx_ctx_load_snapshot(hx_ctx* ctx, const char* path, uint32_t real_bytes);
+
+/* Energy trace in the reference CLI's outputEnergy.txt format
+ * (src/cli_compatibility.cu:80-98): one line "time energy" per entry, both
+ * with 8 significant digits.  Host only. */
+int hx_write_energy_trace(const char* path, const double* times, const double* energies, uint64_t n);
+
 /* Device pointer of the state (hierarchy_size * d * d double2), for callers
  * that fill or read it on the device.  In mixed precision this is the
  * double-precision slab of ADO 0 only (d * d double2).  With Hermitian-packed

@@ -586,4 +586,14 @@ int or_threads(void)
 #endif
 }
 
+// Threads of the following calls (n >= 1).
+void or_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n >= 1) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
 }  // extern "C"

@@ -58,6 +58,7 @@ def lib():
         L.or_trace_distance.restype = C.c_double
         L.or_trace_distance.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         L.or_threads.restype = C.c_int
+        L.or_set_threads.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -100,6 +101,11 @@ def trace_distance(a: np.ndarray, b: np.ndarray) -> float:
 
 def threads() -> int:
     return int(lib().or_threads())
+
+
+def set_threads(n: int) -> None:
+    """OpenMP threads of the following oracle calls."""
+    lib().or_set_threads(int(n))
 
 
 class Oracle:

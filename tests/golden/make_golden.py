@@ -74,10 +74,14 @@ def main() -> None:
     with open(os.path.join(HERE, "reference_legacy_h.json"), "w") as f:
         json.dump(legacy, f)
 
-    trace = np.loadtxt(os.path.join(REF, "examples", "outputEnergy.txt"))
+    trace_path = os.path.join(REF, "examples", "outputEnergy.txt")
+    trace = np.loadtxt(trace_path)
+    with open(trace_path) as f:
+        raw = [ln.rstrip("\n") for ln in f][:200]
     with open(os.path.join(HERE, "legacy_energy_trace.json"), "w") as f:
         json.dump({"source": "reference examples/outputEnergy.txt (FP32, d=1024, dt=0.1)",
-                   "time": trace[:, 0].tolist(), "energy": trace[:, 1].tolist()}, f)
+                   "time": trace[:, 0].tolist(), "energy": trace[:, 1].tolist(),
+                   "lines": raw}, f)
     print("golden fixtures written to", HERE)
 
 

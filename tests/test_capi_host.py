@@ -106,3 +106,15 @@ def test_full_state_flag_is_the_only_flag():
     h = C.c_void_p()
     rc = capi.lib().hx_ctx_create(C.byref(prob), C.byref(h))
     assert rc == 6 and "flags" in capi.lib().hx_last_error().decode()  # InvalidRuntimeOption, no device call
+
+
+def test_energy_trace_writer_matches_the_reference_format(tmp_path, golden):
+    """hx_write_energy_trace writes "time energy" lines with 8 significant
+    digits, like the reference CLI's outputEnergy.txt: the values of the first
+    200 lines of the reference's own file come back as the same text."""
+    lines = golden("legacy_energy_trace.json")["lines"]
+    times = np.array([float(ln.split()[0]) for ln in lines])
+    energies = np.array([float(ln.split()[1]) for ln in lines])
+    path = tmp_path / "outputEnergy.txt"
+    capi.write_energy_trace(str(path), times, energies)
+    assert path.read_text().splitlines() == lines

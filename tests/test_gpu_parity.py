@@ -304,3 +304,51 @@ def test_packed_layout_and_rejection(n):
         xh = _random_state(ctx.size, d, 4, hermitian=True)
         ctx.set_state(xh)
         np.testing.assert_array_equal(ctx.state(), xh)
+
+
+@pytest.mark.parametrize("n", [3, 5])
+def test_snapshot_files_resume_exactly(tmp_path, n):
+    """hx_ctx_save_snapshot / hx_ctx_load_snapshot in the reference's
+    snapshot_rho<N>.dat layout: a double-precision snapshot resumes the run
+    bit for bit (full slabs at d = 8, packed slabs at d = 32); a float one
+    holds the state rounded to float; a file of the wrong size is refused."""
+    p = S.spin_glass(n, seed=61, depth=2, K=1, h=0.9, dt=0.01)
+    with capi.Context(p) as a, capi.Context(p) as b:
+        assert a.hermitian_packed == (p.dim >= 32)
+        a.step(10)
+        a.sync()
+        f8, f4 = str(tmp_path / "snapshot_rho1.dat"), str(tmp_path / "snapshot_rho1f.dat")
+        a.save_snapshot(f8, 8)
+        a.save_snapshot(f4, 4)
+        st = a.state()
+        raw = np.fromfile(f8, np.float64)
+        np.testing.assert_array_equal(raw.view(np.complex128).reshape(st.shape), st)
+        b.load_snapshot(f8, 8)
+        np.testing.assert_array_equal(b.state(), st)
+        a.step(10)
+        b.step(10)
+        a.sync()
+        b.sync()
+        np.testing.assert_array_equal(a.state(), b.state())
+        b.load_snapshot(f4, 4)
+        want = st.astype(np.complex64).astype(np.complex128)
+        if b.hermitian_packed:
+            want = 0.5 * (want + np.conj(np.transpose(want, (0, 2, 1))))
+        np.testing.assert_array_equal(b.state(), want)
+        with pytest.raises(capi.HxError):
+            b.load_snapshot(f4, 8)  # half the bytes a double snapshot needs
+
+
+def test_snapshot_non_hermitian_needs_full_slabs(tmp_path):
+    p = S.spin_glass(5, seed=62, depth=1, K=1)
+    with capi.Context(p, full_state=True) as full, capi.Context(p) as packed:
+        x = _random_state(full.size, p.dim, 5)
+        full.set_state(x)
+        f = str(tmp_path / "snapshot_rho0.dat")
+        full.save_snapshot(f, 8)
+        with pytest.raises(capi.HxError) as err:
+            packed.load_snapshot(f, 8)
+        assert "HX_FLAG_FULL_STATE" in str(err.value)
+        with capi.Context(p, full_state=True) as again:
+            again.load_snapshot(f, 8)
+            np.testing.assert_array_equal(again.state(), x)
