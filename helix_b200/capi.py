@@ -51,17 +51,34 @@ class HxError(RuntimeError):
         super().__init__(f"{self.status}: {message}")
 
 
+class _Csr(C.Structure):
+    _fields_ = [("row_ptr", C.POINTER(C.c_int32)), ("col", C.POINTER(C.c_int32)), ("val", C.POINTER(C.c_double)),
+                ("nnz", C.c_uint32)]
+
+
 class _Bath(C.Structure):
     _fields_ = [("inverse_temperature", C.c_double), ("damping", C.c_double),
                 ("coupling_strength", C.c_double), ("pade_terms", C.c_uint32),
-                ("coupling_diag", C.POINTER(C.c_double)), ("coupling_flip", C.POINTER(C.c_double))]
+                ("coupling_diag", C.POINTER(C.c_double)), ("coupling_flip", C.POINTER(C.c_double)),
+                ("coupling_csr", C.POINTER(_Csr))]
 
 
 class _Problem(C.Structure):
     _fields_ = [("dim", C.c_uint32), ("h_diag", C.POINTER(C.c_double)), ("h_flip", C.POINTER(C.c_double)),
                 ("n_baths", C.c_uint32), ("baths", C.POINTER(_Bath)), ("max_depth", C.c_uint32),
                 ("time_step", C.c_double), ("integration_order", C.c_uint32), ("precision", C.c_uint32),
-                ("flags", C.c_uint32)]
+                ("flags", C.c_uint32), ("h_csr", C.POINTER(_Csr))]
+
+
+def _csr_struct(ptr, col, val, keep):
+    """hx_csr for (row pointers, columns, complex values); arrays kept alive in keep."""
+    p = np.ascontiguousarray(ptr, np.int32)
+    c = np.ascontiguousarray(col, np.int32)
+    v = np.ascontiguousarray(np.asarray(val, np.complex128)).view(np.float64)
+    cs = _Csr(p.ctypes.data_as(C.POINTER(C.c_int32)), c.ctypes.data_as(C.POINTER(C.c_int32)),
+              v.ctypes.data_as(C.POINTER(C.c_double)), int(p[-1]))
+    keep += [p, c, v, cs]
+    return C.pointer(cs)
 
 
 class Info(C.Structure):
@@ -239,8 +256,11 @@ def _problem_struct(problem, order: int = 4, dt: float | None = None, precision:
     keep += [hd, hf]
     baths = (_Bath * len(problem.baths))()
     for j, b in enumerate(problem.baths):
+        if b.v_csr is not None:
+            baths[j] = _Bath(b.beta, b.gamma, b.zeta, b.K, None, None, _csr_struct(*b.v_csr, keep))
+            continue
         if b.v_diag is None:
-            raise HxError(11, "coupling operators must be given as diagonal + per-spin flip weights")
+            raise HxError(11, "a coupling operator needs a diagonal (and flip weights) or a CSR form")
         v = np.ascontiguousarray(b.v_diag, np.float64)
         if v.ndim != 1 or v.shape[0] < d:
             raise HxError(5, "coupling operator dimensions must match the system operator")
@@ -252,11 +272,12 @@ def _problem_struct(problem, order: int = 4, dt: float | None = None, precision:
                 raise HxError(5, "coupling flip weights need one value per spin")
             keep.append(f)
             fp = f.ctypes.data_as(C.POINTER(C.c_double))
-        baths[j] = _Bath(b.beta, b.gamma, b.zeta, b.K, v.ctypes.data_as(C.POINTER(C.c_double)), fp)
+        baths[j] = _Bath(b.beta, b.gamma, b.zeta, b.K, v.ctypes.data_as(C.POINTER(C.c_double)), fp, None)
     keep.append(baths)
+    hc = _csr_struct(*problem.h_csr_explicit, keep) if getattr(problem, "h_csr_explicit", None) is not None else None
     prob = _Problem(d, hd.ctypes.data_as(C.POINTER(C.c_double)), hf.ctypes.data_as(C.POINTER(C.c_double)),
                     len(problem.baths), baths, problem.max_depth, problem.dt if dt is None else dt, order,
-                    precision, flags)
+                    precision, flags, hc)
     return prob, keep
 
 

@@ -142,11 +142,33 @@ Diagnostics validate_solver_options(const SolverOptions& o)
 
 // The executable structure: H = diag(E) + sum_i h_i sx_i (real), each coupling
 // V_j = diag(v_j) + sum_i w_ji sx_i (real).
+struct LoweredCsr {
+    std::vector<int32_t> ptr, col;
+    std::vector<double> val;  // re, im interleaved
+};
+
 struct Lowered {
     uint32_t dim = 0;
     std::vector<double> hdiag, hflip;
     std::vector<std::vector<double>> vdiag, vflip;
+    // operators outside the diagonal-plus-flip structure, passed on in CSR form
+    bool h_is_csr = false;
+    LoweredCsr hcsr;
+    std::vector<LoweredCsr> vcsr;  // per coupling; empty ptr = diagonal-plus-flip form
 };
+
+LoweredCsr csr_of(const SparseOperator& op)
+{
+    LoweredCsr o;
+    o.ptr.reserve(op.rowOffsets.size());
+    for (std::size_t x : op.rowOffsets) o.ptr.push_back(static_cast<int32_t>(x));
+    for (std::size_t c : op.columnIndices) o.col.push_back(static_cast<int32_t>(c));
+    for (const std::complex<double>& v : op.values) {
+        o.val.push_back(v.real());
+        o.val.push_back(v.imag());
+    }
+    return o;
+}
 
 // Split a real CSR operator into its diagonal and per-spin flip weights;
 // false if it has any other structure.
@@ -234,6 +256,8 @@ bool lower_system(const System& s, Lowered& out, std::string& why)
     int n = 0;
     while ((std::size_t(1) << n) < d) ++n;
     out.dim = static_cast<uint32_t>(d);
+    // H as diagonal plus uniform single-spin flips (the fused kernels), else in CSR
+    auto flip_form = [&](std::string& why) {
     out.hdiag.assign(d, 0.0);
     out.hflip.assign(n, 0.0);
     std::vector<bool> seen(n, false);
@@ -277,12 +301,25 @@ bool lower_system(const System& s, Lowered& out, std::string& why)
                 }
             }
         }
+    return true;
+    };
+    std::string why_h;
+    out.h_is_csr = !flip_form(why_h);
+    if (out.h_is_csr) out.hcsr = csr_of(H);
     out.vdiag.clear();
     out.vflip.clear();
+    out.vcsr.clear();
     for (std::size_t k = 0; k < s.couplings.size(); ++k) {
         std::vector<double> v, w;
         const std::string name = "coupling[" + std::to_string(k) + "]";
-        if (!split_flip_operator(s.couplings[k], d, n, v, w, why, name.c_str())) return false;
+        std::string why_v;
+        if (split_flip_operator(s.couplings[k], d, n, v, w, why_v, name.c_str())) {
+            out.vcsr.emplace_back();
+        } else {
+            v.assign(d, 0.0);
+            w.assign(n, 0.0);
+            out.vcsr.push_back(csr_of(s.couplings[k]));
+        }
         out.vdiag.push_back(std::move(v));
         out.vflip.push_back(std::move(w));
     }
@@ -442,6 +479,8 @@ public:
     {
         if (ctx_) return;
         std::vector<hx_bath> baths(sys.vdiag.size());
+        std::vector<hx_csr> vcsr(sys.vdiag.size());
+        hx_csr hcsr{};
         for (std::size_t j = 0; j < baths.size(); ++j) {
             const Bath& b = hier.baths.size() == 1 ? hier.baths[0] : hier.baths[j];
             baths[j].inverse_temperature = b.inverseTemperature;
@@ -450,11 +489,21 @@ public:
             baths[j].pade_terms = static_cast<uint32_t>(b.padeTerms);
             baths[j].coupling_diag = sys.vdiag[j].data();
             baths[j].coupling_flip = sys.vflip.size() > j ? sys.vflip[j].data() : nullptr;
+            if (sys.vcsr.size() > j && !sys.vcsr[j].ptr.empty()) {
+                const LoweredCsr& o = sys.vcsr[j];
+                vcsr[j] = hx_csr{o.ptr.data(), o.col.data(), o.val.data(), static_cast<uint32_t>(o.col.size())};
+                baths[j].coupling_csr = &vcsr[j];
+            }
         }
         hx_problem p{};
         p.dim = sys.dim;
         p.h_diag = sys.hdiag.data();
         p.h_flip = sys.hflip.data();
+        if (sys.h_is_csr) {
+            hcsr = hx_csr{sys.hcsr.ptr.data(), sys.hcsr.col.data(), sys.hcsr.val.data(),
+                          static_cast<uint32_t>(sys.hcsr.col.size())};
+            p.h_csr = &hcsr;
+        }
         p.n_baths = static_cast<uint32_t>(baths.size());
         p.baths = baths.data();
         p.max_depth = static_cast<uint32_t>(hier.maxDepth);

@@ -953,6 +953,7 @@ int hx_batch_create(const hx_problem* problems, uint32_t count, const hx_batch_o
         if (d < 2 || (d & (d - 1)) != 0 || d > 64)
             return fail(HX_ERR_INVALID_DIMENSION, "batched instances need dim = 2^k with 2 <= dim <= 64");
         if (!p.h_diag) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "h_diag is NULL");
+        if (p.h_csr) return fail(HX_ERR_UNSUPPORTED_EXECUTION, "batched instances take diagonal plus flip Hamiltonians");
         if (p.precision != HX_PRECISION_DOUBLE) return fail(HX_ERR_UNSUPPORTED_PRECISION, "batches propagate in double precision");
         if (p.time_step != dt || p.integration_order != order)
             return fail(HX_ERR_INVALID_RUNTIME_OPTION, "all instances of a batch share time_step and integration_order");
@@ -963,7 +964,8 @@ int hx_batch_create(const hx_problem* problems, uint32_t count, const hx_batch_o
         if ((p.flags & ~HX_FLAG_FULL_STATE) != 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "unknown flags");
         for (uint32_t j = 0; j < p.n_baths; ++j) {
             const hx_bath& bb = p.baths[j];
-            if (!bb.coupling_diag) return fail(HX_ERR_UNSUPPORTED_BATH, "bath coupling operator is NULL");
+            if (!bb.coupling_diag || bb.coupling_csr)
+                return fail(HX_ERR_UNSUPPORTED_BATH, "batched instances need sigma_z coupling diagonals");
             if (bb.coupling_flip)
                 for (uint32_t k = 0; (1u << k) < d; ++k)
                     if (bb.coupling_flip[k] != 0.0)

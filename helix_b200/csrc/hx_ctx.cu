@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
 #include <thread>
@@ -55,7 +56,8 @@ void release(hx_ctx* c)
                     c->trace_buf, c->energy_buf, c->diag_table, c->ent_count, c->ent_slab, c->ent_bath,
                     c->ent_wc, c->ent_wa, c->order_perm, c->ado_keep, c->up_slot, c->up_ado, c->up_cnt,
                     c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf, c->rho32, c->ua32, c->ub32,
-                    c->U32, c->diag32, c->vdiag32, c->hflip32, c->diag_herm, c->vbit};
+                    c->U32, c->diag32, c->vdiag32, c->hflip32, c->diag_herm, c->vbit, c->csr_ptr, c->csr_col,
+                    c->csr_val};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -267,6 +269,12 @@ int launch_stage_any(hx_ctx* c, const double2* u, const double2* rho, double2* o
 int launch_stage_core(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
 {
     if (c->use_large) return launch_large_stage(c, u, rho, out, alpha, base);
+    if (c->use_csr) {
+        const hx::CsrArgs a{c->csr_ptr, c->csr_col, c->csr_val, c->edges, c->acoef, c->bcoef, c->gsum,
+                            c->xi,      c->counter, c->bath_off, c->H, c->M, c->J, c->logd};
+        hx::launch_csr_stage(a, u, c->Bbuf, rho, out, alpha, base, c->stream);
+        return 2;
+    }
     if (c->use_flip) {
         hx::launch_flip_stage(flip_args_of(c), u, c->Bbuf, rho, out, alpha, base, c->stream);
         return 2;
@@ -306,6 +314,13 @@ int enqueue_step(hx_ctx* c)
     c->counters.stage_launches += m;
     c->steps_done += 1;
     return HX_OK;
+}
+
+// Energy and trace of rho_0 into out[0..2].
+void launch_obs(hx_ctx* c, double* out)
+{
+    if (c->use_csr) hx::launch_observables_csr(c->rho, c->logd, c->csr_ptr, c->csr_col, c->csr_val, out, c->stream);
+    else hx::launch_observables(c->rho, c->logd, c->herm, c->hdiag, c->hflip, nullptr, out, c->stream);
 }
 
 int check_launch(const char* what)
@@ -397,6 +412,84 @@ int read_herm(hx_ctx* c, const double2* src, size_t count, double* out)
     return HX_OK;
 }
 
+// One operator in compressed rows, host side, before upload.
+struct HostCsr {
+    std::vector<int32_t> ptr;  // d + 1, relative
+    std::vector<int32_t> col;
+    std::vector<double2> val;
+};
+
+// Copy and check a caller's CSR operator: row pointers from 0 to nnz and
+// non-decreasing, columns in range, values finite, Hermitian to 1e-12 of its
+// largest entry (duplicates summed).
+bool take_csr(const hx_csr* a, int d, HostCsr& out, std::string& why, const std::string& name)
+{
+    if (!a->row_ptr || (a->nnz > 0 && (!a->col || !a->val))) {
+        why = name + ": NULL array";
+        return false;
+    }
+    if (a->row_ptr[0] != 0 || a->row_ptr[d] != static_cast<int32_t>(a->nnz)) {
+        why = name + ": row pointers must run from 0 to nnz";
+        return false;
+    }
+    out.ptr.assign(a->row_ptr, a->row_ptr + d + 1);
+    out.col.assign(a->col, a->col + a->nnz);
+    out.val.resize(a->nnz);
+    std::map<std::pair<int, int>, std::pair<double, double>> sum;
+    double big = 0.0;
+    for (int r = 0; r < d; ++r) {
+        if (out.ptr[r + 1] < out.ptr[r]) {
+            why = name + ": row pointers decrease";
+            return false;
+        }
+        for (int q = out.ptr[r]; q < out.ptr[r + 1]; ++q) {
+            const int c = out.col[q];
+            const double re = a->val[2 * q], im = a->val[2 * q + 1];
+            if (c < 0 || c >= d) {
+                why = name + ": column index out of range";
+                return false;
+            }
+            if (!std::isfinite(re) || !std::isfinite(im)) {
+                why = name + ": value is not finite";
+                return false;
+            }
+            out.val[q] = make_double2(re, im);
+            auto& v = sum[{r, c}];
+            v.first += re;
+            v.second += im;
+        }
+    }
+    for (const auto& kv : sum) big = std::max(big, std::hypot(kv.second.first, kv.second.second));
+    const double tol = 1e-12 * std::max(big, 1e-300);
+    for (const auto& kv : sum) {
+        const auto it = sum.find({kv.first.second, kv.first.first});
+        const double tr = it == sum.end() ? 0.0 : it->second.first, ti = it == sum.end() ? 0.0 : -it->second.second;
+        if (std::hypot(kv.second.first - tr, kv.second.second - ti) > tol) {
+            why = name + ": operator is not Hermitian";
+            return false;
+        }
+    }
+    return true;
+}
+
+// CSR of diag(v) + sum_i w_i sigma_x(i).
+HostCsr flip_csr(const double* v, const double* w, int d, int logd)
+{
+    HostCsr o;
+    o.ptr.push_back(0);
+    for (int r = 0; r < d; ++r) {
+        o.col.push_back(r);
+        o.val.push_back(make_double2(v ? v[r] : 0.0, 0.0));
+        for (int i = 0; w && i < logd; ++i)
+            if (w[i] != 0.0) {
+                o.col.push_back(r ^ (1 << i));
+                o.val.push_back(make_double2(w[i], 0.0));
+            }
+        o.ptr.push_back(static_cast<int32_t>(o.col.size()));
+    }
+    return o;
+}
+
 // Mixed precision: the whole state as complex128 on the host (complex64
 // hierarchy widened, ADO 0 from its double-precision slab); src32/src64 are
 // matching buffers (rho32/rho, ua32/ua, ...).
@@ -472,7 +565,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     while ((1u << logd) < d) ++logd;
     if (logd > hx::kMaxLogDFlip)
         return fail(HX_ERR_UNSUPPORTED_EXECUTION, "dim must be at most 4096");
-    if (!p->h_diag) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "h_diag is NULL");
+    if (!p->h_diag && !p->h_csr) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "h_diag is NULL");
     if (p->precision != HX_PRECISION_DOUBLE && p->precision != HX_PRECISION_MIXED)
         return fail(HX_ERR_UNSUPPORTED_PRECISION, "precision must be HX_PRECISION_DOUBLE or HX_PRECISION_MIXED");
     if (p->precision == HX_PRECISION_MIXED && (logd < 7 || logd > 10 || p->max_depth < 3))
@@ -487,11 +580,38 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     if ((p->flags & ~HX_FLAG_FULL_STATE) != 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "unknown flags");
 
     const int J = static_cast<int>(p->n_baths);
+    // general sparse operators: checked and gathered here, run on the CSR path
+    bool use_csr = p->h_csr != nullptr;
+    for (int j = 0; j < J; ++j) use_csr = use_csr || p->baths[j].coupling_csr != nullptr;
+    std::vector<HostCsr> ops;
+    if (use_csr) {
+        if (p->precision != HX_PRECISION_DOUBLE)
+            return fail(HX_ERR_UNSUPPORTED_PRECISION, "sparse operators run in double precision");
+        std::string why;
+        ops.resize(J + 1);
+        if (p->h_csr) {
+            if (!take_csr(p->h_csr, static_cast<int>(d), ops[0], why, "h_csr"))
+                return fail(HX_ERR_INVALID_RUNTIME_OPTION, why);
+        } else {
+            ops[0] = flip_csr(p->h_diag, p->h_flip, static_cast<int>(d), logd);
+        }
+        for (int j = 0; j < J; ++j) {
+            const hx_bath& b = p->baths[j];
+            if (b.coupling_csr) {
+                if (!take_csr(b.coupling_csr, static_cast<int>(d), ops[1 + j], why,
+                              "coupling_csr[" + std::to_string(j) + "]"))
+                    return fail(HX_ERR_UNSUPPORTED_BATH, why);
+            } else {
+                if (!b.coupling_diag) return fail(HX_ERR_UNSUPPORTED_BATH, "bath coupling operator is NULL");
+                ops[1 + j] = flip_csr(b.coupling_diag, b.coupling_flip, static_cast<int>(d), logd);
+            }
+        }
+    }
     std::vector<hx::BathConst> bc(J);
     int M = 0;
     for (int j = 0; j < J; ++j) {
         const hx_bath& b = p->baths[j];
-        if (!b.coupling_diag) return fail(HX_ERR_UNSUPPORTED_BATH, "bath coupling operator is NULL");
+        if (!b.coupling_diag && !b.coupling_csr) return fail(HX_ERR_UNSUPPORTED_BATH, "bath coupling operator is NULL");
         if (!(b.inverse_temperature > 0.0) || !(b.damping > 0.0) || !std::isfinite(b.coupling_strength))
             return fail(HX_ERR_UNSUPPORTED_BATH, "bath needs positive beta and gamma and a finite coupling");
         if (b.pade_terms > 32) return fail(HX_ERR_UNSUPPORTED_BATH, "too many Pade terms");
@@ -531,29 +651,44 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     std::vector<double> vf(static_cast<size_t>(J) * logd, 0.0);
     bool any_flip = false;
     for (int j = 0; j < J; ++j)
-        if (p->baths[j].coupling_flip)
+        if (p->baths[j].coupling_flip && !p->baths[j].coupling_csr)
             for (int i = 0; i < logd; ++i) {
                 const double w = p->baths[j].coupling_flip[i];
-                if (!std::isfinite(w)) return fail(HX_ERR_UNSUPPORTED_BATH, "coupling flip weight is not finite");
+                if (!std::isfinite(w)) return bail(fail(HX_ERR_UNSUPPORTED_BATH, "coupling flip weight is not finite"));
                 vf[static_cast<size_t>(j) * logd + i] = w;
                 any_flip = any_flip || w != 0.0;
             }
-    c->use_large = !any_flip && logd >= 7 && hx::large_supported(logd, M, J);
-    c->use_flip = any_flip || (logd > hx::kMaxLogD && !c->use_large);
+    c->use_csr = use_csr;
+    c->use_large = !use_csr && !any_flip && logd >= 7 && hx::large_supported(logd, M, J);
+    c->use_flip = !use_csr && (any_flip || (logd > hx::kMaxLogD && !c->use_large));
     c->mixed = p->precision == HX_PRECISION_MIXED;
     if (c->mixed && !c->use_large)
         return bail(fail(HX_ERR_UNSUPPORTED_PRECISION, "mixed precision needs diagonal coupling operators"));
     // fused stage kernels (d = 32, 64), on Hermitian-packed slabs unless the caller keeps full slabs
     const char* force_generic = std::getenv("HX_FORCE_GENERIC_STAGE");
     const bool want_herm = (p->flags & HX_FLAG_FULL_STATE) == 0;
-    const bool fused_ok = !c->use_flip && !c->use_large && logd >= 5 && logd <= hx::kMaxLogD &&
+    const bool fused_ok = !c->use_flip && !c->use_large && !c->use_csr && logd >= 5 && logd <= hx::kMaxLogD &&
                           hx::fused_supported(logd, M, J, want_herm ? 1 : 0) &&
                           !(force_generic && force_generic[0] == '1');
     c->herm = fused_ok && want_herm;
     c->slab_store = c->herm ? static_cast<size_t>(hx::herm_elems(logd)) : c->slab;
     const size_t nstate = static_cast<size_t>(H) * c->slab_store;
     if ((rc = dev_alloc(c, &c->vflip, vf.size())) || (rc = upload(c, c->vflip, vf))) return bail(rc);
-    if (c->use_flip && (rc = dev_alloc(c, &c->Bbuf, nstate * J))) return bail(rc);
+    if ((c->use_flip || c->use_csr) && (rc = dev_alloc(c, &c->Bbuf, nstate * J))) return bail(rc);
+    if (c->use_csr) {
+        std::vector<int32_t> ptr, col;
+        std::vector<double2> val;
+        for (const HostCsr& o : ops) {
+            const int32_t base = static_cast<int32_t>(col.size());
+            for (int32_t x : o.ptr) ptr.push_back(base + x);
+            col.insert(col.end(), o.col.begin(), o.col.end());
+            val.insert(val.end(), o.val.begin(), o.val.end());
+        }
+        if ((rc = dev_alloc(c, &c->csr_ptr, ptr.size())) || (rc = dev_alloc(c, &c->csr_col, col.size())) ||
+            (rc = dev_alloc(c, &c->csr_val, val.size())) || (rc = upload(c, c->csr_ptr, ptr)) ||
+            (rc = upload(c, c->csr_col, col)) || (rc = upload(c, c->csr_val, val)))
+            return bail(rc);
+    }
     // double-precision state: the whole hierarchy, or only ADO 0 in mixed precision
     const size_t n64 = c->mixed ? c->slab : nstate;
     if (c->mixed && ((rc = dev_alloc(c, &c->rho32, nstate)) || (rc = dev_alloc(c, &c->ua32, nstate)) ||
@@ -569,14 +704,24 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
         (rc = dev_alloc(c, &c->error_flag, 1)) || (rc = dev_alloc(c, &c->obs, 4)))
         return bail(rc);
 
-    // host-side operator data
-    c->h_hdiag.assign(p->h_diag, p->h_diag + d);
+    // host-side operator data (with sparse operators: the real parts of their diagonals)
+    auto diag_of = [&](const HostCsr& o, double* outd) {
+        for (uint32_t r = 0; r < d; ++r) {
+            outd[r] = 0.0;
+            for (int q = o.ptr[r]; q < o.ptr[r + 1]; ++q)
+                if (o.col[q] == static_cast<int32_t>(r)) outd[r] += o.val[q].x;
+        }
+    };
+    c->h_hdiag.assign(d, 0.0);
+    if (p->h_csr) diag_of(ops[0], c->h_hdiag.data());
+    else c->h_hdiag.assign(p->h_diag, p->h_diag + d);
     c->h_hflip.assign(logd, 0.0);
-    if (p->h_flip) c->h_hflip.assign(p->h_flip, p->h_flip + logd);
+    if (p->h_flip && !p->h_csr) c->h_hflip.assign(p->h_flip, p->h_flip + logd);
     std::vector<double> vd(static_cast<size_t>(J) * d), xi(J), ct(J), nu_m(M), phi_m(M, 0.0), tc(J), ta(J);
     std::vector<int32_t> off(J + 1), mb(M), mk(M);
     for (int j = 0; j < J; ++j) {
-        std::copy(p->baths[j].coupling_diag, p->baths[j].coupling_diag + d, vd.begin() + static_cast<size_t>(j) * d);
+        if (p->baths[j].coupling_csr) diag_of(ops[1 + j], vd.data() + static_cast<size_t>(j) * d);
+        else std::copy(p->baths[j].coupling_diag, p->baths[j].coupling_diag + d, vd.begin() + static_cast<size_t>(j) * d);
         xi[j] = bc[j].xi;
         ct[j] = bc[j].counter;
         tc[j] = bc[j].theta_c;
@@ -754,7 +899,7 @@ int hx_ctx_info(const hx_ctx* c, hx_info* info)
     info->device_bytes = c->device_bytes;
     info->steps_done = c->steps_done;
     info->time = static_cast<double>(c->steps_done) * c->dt;
-    int per_stage = (c->use_flip || (c->use_fused && c->up_slots > 0)) ? 2 : 1;
+    int per_stage = (c->use_flip || c->use_csr || (c->use_fused && c->up_slots > 0)) ? 2 : 1;
     if (c->use_large) per_stage = 1 + (c->up_slots > 0 ? 1 : 0) + (c->mixed ? 1 : 0);
     info->kernels_per_step = static_cast<uint32_t>(c->order) * per_stage;
     return HX_OK;
@@ -808,8 +953,7 @@ int hx_ctx_step_trace(hx_ctx* c, uint64_t nsteps, double* rho0_trace, double* en
         const int chunk = static_cast<int>(std::min<uint64_t>(nsteps - done, c->trace_cap));
         for (int t = 0; t < chunk; ++t) {
             enqueue_step(c);
-            hx::launch_observables(c->rho, c->logd, c->herm, c->hdiag, c->hflip, nullptr, c->energy_buf + 3 * t,
-                                   c->stream);
+            launch_obs(c, c->energy_buf + 3 * t);
             c->counters.kernel_launches += 1;
             if (rho0_trace)
                 HX_CUDA_TRY(cudaMemcpyAsync(c->trace_buf + static_cast<size_t>(t) * c->slab_store, c->rho,
@@ -859,7 +1003,7 @@ int hx_ctx_read_rho0(hx_ctx* c, double* out, uint64_t n)
 int hx_ctx_observables(hx_ctx* c, double* energy, double* trace_re, double* trace_im)
 {
     if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
-    hx::launch_observables(c->rho, c->logd, c->herm, c->hdiag, c->hflip, nullptr, c->obs, c->stream);
+    launch_obs(c, c->obs);
     c->counters.kernel_launches += 1;
     int rc = check_launch("observables kernel");
     if (rc != HX_OK) return rc;
@@ -1043,7 +1187,7 @@ int hx_ctx_set_closure(hx_ctx* c, hx_closure* cl)
     if (cl) {
         uint32_t top = 0;
         hx_closure_info(cl, &top, nullptr, nullptr, nullptr, nullptr);
-        if (c->mixed || c->use_flip || c->use_large || c->d > 64)
+        if (c->mixed || c->use_flip || c->use_large || c->use_csr || c->d > 64)
             return fail(HX_ERR_UNSUPPORTED_EXECUTION, "closures run with double precision and dim <= 64");
         if (!hx::closure_matches_hierarchy(cl, c->d, c->M, c->H))
             return fail(HX_ERR_INVALID_RUNTIME_OPTION, "the closure was made for another hierarchy");

@@ -253,6 +253,29 @@ struct FlipArgs {
 void launch_flip_stage(const FlipArgs& a, const double2* u, double2* B, const double2* rho, double2* out,
                        double alpha, int base_kind, cudaStream_t s);
 
+// Two-pass stage for general sparse Hermitian H and V_j (hx_csr.cu).
+// Operator k (0 = H, 1 + j = V_j) has row pointers ptr[k (d+1) .. k (d+1) + d]
+// (absolute offsets into col / val).
+struct CsrArgs {
+    const int32_t* ptr;      // [(J+1)(d+1)]
+    const int32_t* col;
+    const double2* val;
+    const int32_t* edges;    // [H][2M]
+    const double* acoef;     // [H][M]
+    const double* bcoef;     // [H][J]
+    const double* gsum;      // [H]
+    const double* xi;        // [J]
+    const double* counter;   // [J]
+    const int32_t* bath_off; // [J+1]
+    long long H;
+    int M, J, logd;
+};
+void launch_csr_stage(const CsrArgs& a, const double2* u, double2* B, const double2* rho, double2* out, double alpha,
+                      int base_kind, cudaStream_t s);
+// out[0] = Re Tr(H rho_0) with H in CSR (operator 0), out[1..2] = Tr rho_0.
+void launch_observables_csr(const double2* rho0, int logd, const int32_t* ptr, const int32_t* col,
+                            const double2* val, double* out, cudaStream_t s);
+
 // Tables on the device (hx_tables.cu)
 int build_tables_device(int M, int D, long long H, int32_t* d_rows, int32_t* d_edges, cudaStream_t s);
 // Same table kernel with a binomial table (rows n <= M + D, columns k <= M,
@@ -301,6 +324,10 @@ struct hx_ctx {
     double* vdiag = nullptr;
     double* vflip = nullptr;      // [J][log2 d]
     bool use_flip = false;        // two-pass flip path (flips in V, or d > 1024)
+    bool use_csr = false;         // two-pass path for general sparse H / V_j (hx_csr.cu)
+    int32_t* csr_ptr = nullptr;   // [(J+1)(d+1)] operator 0 = H, 1 + j = V_j
+    int32_t* csr_col = nullptr;
+    double2* csr_val = nullptr;
     bool use_large = false;       // band kernels for 128 <= d <= 1024, diagonal V (hx_large.cu)
     bool mixed = false;           // complex64 hierarchy, ADO 0 in double precision
     hx_closure* closure = nullptr; // learned closure term added by every stage (hx_mlp.cu)

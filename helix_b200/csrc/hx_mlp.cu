@@ -901,6 +901,10 @@ int hx_closure_create(const hx_problem* coarse, uint32_t fine_max_depth, uint32_
     *out = nullptr;
     if (!coarse || !coarse->baths || coarse->n_baths == 0 || !coarse->h_diag)
         return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL problem");
+    if (coarse->h_csr) return fail(HX_ERR_UNSUPPORTED_EXECUTION, "closures need diagonal plus flip Hamiltonians");
+    for (uint32_t j = 0; j < coarse->n_baths; ++j)
+        if (coarse->baths[j].coupling_csr)
+            return fail(HX_ERR_UNSUPPORTED_EXECUTION, "closures need diagonal coupling operators");
     const uint32_t d = coarse->dim;
     if (d < 2 || d > 64 || (d & (d - 1)) != 0) return fail(HX_ERR_INVALID_DIMENSION, "closures need 2 <= dim <= 64");
     if (coarse->max_depth < 2 || fine_max_depth <= coarse->max_depth)

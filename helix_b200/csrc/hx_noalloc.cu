@@ -93,6 +93,10 @@ extern "C" int hx_rhs_noalloc(const hx_problem* p, const double* rho_device, dou
     if (p->max_depth < 1) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "max_depth must be >= 1");
 
     const int J = static_cast<int>(p->n_baths);
+    if (p->h_csr) return fail(HX_ERR_UNSUPPORTED_EXECUTION, "hx_rhs_noalloc takes diagonal plus flip Hamiltonians only");
+    for (int j = 0; j < J; ++j)
+        if (p->baths[j].coupling_csr)
+            return fail(HX_ERR_UNSUPPORTED_BATH, "hx_rhs_noalloc supports diagonal coupling operators only");
     for (int j = 0; j < J; ++j)
         if (p->baths[j].coupling_flip)
             for (int i = 0; i < logd; ++i)

@@ -115,6 +115,7 @@ class Problem:
     dt: float
     name: str = ""
     meta: dict = field(default_factory=dict)
+    h_csr_explicit: tuple | None = None  # (ptr, col, complex val): a general H in place of h_diag / h_flip
 
     @property
     def n_spins(self) -> int:
@@ -129,6 +130,9 @@ class Problem:
 
     def h_csr(self):
         """H as CSR (ptr, col, complex val), row-major, columns ascending."""
+        if self.h_csr_explicit is not None:
+            ptr, col, val = self.h_csr_explicit
+            return np.asarray(ptr, np.int32), np.asarray(col, np.int32), np.asarray(val, np.complex128)
         d = self.dim
         n = self.n_spins
         ptr = [0]
@@ -347,3 +351,47 @@ def initial_rho0(dim: int) -> np.ndarray:
     rho = np.zeros((dim, dim), np.complex128)
     rho[dim - 1, dim - 1] = 1.0
     return rho
+
+
+def random_hermitian_csr(dim: int, per_row: int, seed: int, scale: float = 1.0):
+    """Seeded sparse complex Hermitian operator in CSR (ptr, col, val): a real
+    diagonal plus per_row random off-diagonal pairs per row, values from
+    splitmix64 uniforms in (-scale, scale)."""
+    rng = SplitMix64(seed)
+    entries: dict[tuple[int, int], complex] = {}
+    for r in range(dim):
+        entries[(r, r)] = entries.get((r, r), 0.0) + scale * (2.0 * rng.uniform() - 1.0)
+        for _ in range(per_row):
+            c = int(rng.uniform() * dim) % dim
+            if c == r:
+                continue
+            v = complex(scale * (2.0 * rng.uniform() - 1.0), scale * (2.0 * rng.uniform() - 1.0))
+            entries[(r, c)] = entries.get((r, c), 0.0) + v
+            entries[(c, r)] = entries.get((c, r), 0.0) + v.conjugate()
+    ptr, col, val = [0], [], []
+    for r in range(dim):
+        row = sorted((c, v) for (rr, c), v in entries.items() if rr == r)
+        for c, v in row:
+            col.append(c)
+            val.append(v)
+        ptr.append(len(col))
+    return np.array(ptr, np.int32), np.array(col, np.int32), np.array(val, np.complex128)
+
+
+def sparse_problem(n_spins: int, seed: int, depth: int = 2, K: int = 1, lam: float = 0.1, gamma: float = 1.0,
+                   temperature: float = 1.0, dt: float = 0.01, per_row: int = 3) -> Problem:
+    """A general sparse instance (System::from_sparse style): random sparse
+    complex Hermitian H and one random sparse Hermitian coupling operator per
+    spin, each bath Drude-Lorentz with K Pade terms."""
+    d = 1 << n_spins
+    h = random_hermitian_csr(d, per_row, seed)
+    baths = [BathSpec.drude_lorentz(lam, gamma, temperature, K,
+                                    v_csr=random_hermitian_csr(d, 2, seed * 1000 + 17 * (i + 1), 0.5))
+             for i in range(n_spins)]
+    diag = np.zeros(d)
+    for r in range(d):
+        for q in range(h[0][r], h[0][r + 1]):
+            if h[1][q] == r:
+                diag[r] += h[2][q].real
+    return Problem(dim=d, h_diag=diag, h_flip=np.zeros(n_spins), baths=baths, max_depth=depth + 1, dt=dt,
+                   name=f"sparse_n{n_spins}_s{seed}", h_csr_explicit=h)

@@ -53,6 +53,17 @@ extern "C" {
  * precision is fixed at compile time (src/legacy_compile_options.h:6). */
 #define HX_PRECISION_MIXED 2
 
+/* A sparse d x d complex operator in compressed rows: row r holds the entries
+ * row_ptr[r] .. row_ptr[r+1]-1, entry p in column col[p] with value
+ * val[2p] + i val[2p+1].  (The reference's SparseOperator,
+ * include/helix/types.h:122-128, with 32-bit indices.) */
+typedef struct hx_csr {
+    const int32_t* row_ptr;     /* d + 1 */
+    const int32_t* col;         /* nnz */
+    const double* val;          /* 2 nnz */
+    uint32_t nnz;
+} hx_csr;
+
 /* One Drude-Lorentz bath with Pade terms, coupled through the system operator
  * V_j = diag(coupling_diag) + sum_i coupling_flip[i] * sigma_x(spin i).
  * Replaces the compiled bath and coupling operator of the reference
@@ -65,6 +76,7 @@ typedef struct hx_bath {
     uint32_t pade_terms;        /* K (Param::KMax) */
     const double* coupling_diag; /* dim real values: diagonal of V_j */
     const double* coupling_flip; /* log2(dim) real values (sigma_x weights of V_j), or NULL */
+    const hx_csr* coupling_csr;  /* or NULL; a general Hermitian V_j, in place of coupling_diag / _flip */
 } hx_bath;
 
 /* One HEOM problem.  H = diag(h_diag) + sum_i h_flip[i] * sigma_x(spin i),
@@ -81,7 +93,15 @@ typedef struct hx_problem {
     uint32_t integration_order; /* Taylor order (Param::IntegrationNum), 1..8 */
     uint32_t precision;         /* HX_PRECISION_DOUBLE or HX_PRECISION_MIXED */
     uint32_t flags;             /* 0 or HX_FLAG_FULL_STATE */
+    const hx_csr* h_csr;        /* or NULL; a general Hermitian H, in place of h_diag / h_flip */
 } hx_problem;
+
+/* General sparse operators (h_csr, coupling_csr; the reference validates
+ * System::from_sparse but does not execute it, src/helix.cpp:166-258,335-347)
+ * run on a two-pass stage that gathers along the CSR rows of H and V_j
+ * (d <= 4096, double precision, full slabs).  Both must be Hermitian to 1e-12
+ * of their largest entry; batches, closures, mixed precision and
+ * hx_rhs_noalloc take diagonal / flip operators only. */
 
 /* Every ADO of this hierarchy stays Hermitian (H and the V_j are Hermitian
  * and every term of the right-hand side maps Hermitian matrices to Hermitian

@@ -2,10 +2,14 @@
 // (helix::HEOMSolver(options).run(system, hierarchy, solverOptions)) and
 // prints the result as JSON for tests/test_cpp_api.py to check against the
 // FP64 oracle.  Usage: api_spin_glass <spins> <seed> <h> <depth> <K> <steps> <dt> <mode>
-//   mode: final | trace | trajectory | single | legacy | sparse-bad
+//   mode: final | trace | trajectory | single | legacy | sparse-bad | sparse-general
 #include <helix/helix.h>
 
+#include <algorithm>
+#include <complex>
 #include <cstdio>
+#include <utility>
+#include <vector>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -37,6 +41,29 @@ int main(int argc, char** argv)
         system = helix::examples::legacy_spin_glass_system();
         hierarchy = helix::HierarchySpec::compiled_default(helix::Bath::drude_lorentz_pade());
         options = helix::ContextOptions{};
+    }
+    if (mode == "sparse-general") {
+        // H plus the complex Hermitian two-spin term 0.05 i (|r><r^3| - |r^3><r|), r < r^3:
+        // outside the diagonal-plus-flip form, so System::from_sparse runs on the CSR path
+        const helix::SparseOperator& H0 = system.hamiltonian;
+        helix::SparseOperator H = H0;
+        H.rowOffsets.assign(1, 0);
+        H.columnIndices.clear();
+        H.values.clear();
+        for (std::size_t r = 0; r < H0.rows; ++r) {
+            std::vector<std::pair<std::size_t, std::complex<double>>> row;
+            for (std::size_t p = H0.rowOffsets[r]; p < H0.rowOffsets[r + 1]; ++p)
+                row.emplace_back(H0.columnIndices[p], H0.values[p]);
+            const std::size_t s = r ^ 3u;
+            row.emplace_back(s, std::complex<double>(0.0, r < s ? 0.05 : -0.05));
+            std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            for (const auto& e : row) {
+                H.columnIndices.push_back(e.first);
+                H.values.push_back(e.second);
+            }
+            H.rowOffsets.push_back(H.columnIndices.size());
+        }
+        system = helix::System::from_sparse(H, system.couplings);
     }
     if (mode == "sparse-bad") {
         // a column index outside the operator: System::from_sparse validation must flag it

@@ -118,3 +118,28 @@ def test_energy_trace_writer_matches_the_reference_format(tmp_path, golden):
     path = tmp_path / "outputEnergy.txt"
     capi.write_energy_trace(str(path), times, energies)
     assert path.read_text().splitlines() == lines
+
+
+def test_sparse_operator_validation_before_any_device_call():
+    """General sparse H / V (hx_csr) are checked on the host: Hermitian,
+    columns in range, double precision only."""
+    good = S.sparse_problem(3, seed=5)
+    bad = S.sparse_problem(3, seed=5)
+    ptr, col, val = bad.h_csr_explicit
+    val = val.copy()
+    off = next(q for q in range(len(col)) if col[q] != 0 and ptr[0] <= q < ptr[1])  # an off-diagonal of row 0
+    val[off] += 0.5j
+    bad.h_csr_explicit = (ptr, col, val)
+    assert _status_of(bad) == "InvalidRuntimeOption"
+    bad2 = S.sparse_problem(3, seed=5)
+    p2, c2, v2 = bad2.baths[0].v_csr
+    c2 = c2.copy()
+    c2[0] = 99
+    bad2.baths[0].v_csr = (p2, c2, v2)
+    assert _status_of(bad2) == "UnsupportedBath"
+    prob, keep = capi._problem_struct(good, precision=capi.PRECISION_MIXED)
+    h = C.c_void_p()
+    assert capi.lib().hx_ctx_create(C.byref(prob), C.byref(h)) == 7  # UnsupportedPrecision
+    o = O.Oracle(good)  # the oracle takes the same operators
+    assert o.size == good.hierarchy_size()
+    o.close()
