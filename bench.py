@@ -571,7 +571,8 @@ def run_mixed(args, cfg: dict) -> None:
     H = int(info.hierarchy_size)
     value = H * args.steps / (ms / 1000.0)
     plain = H * args.steps / (ms64 / 1000.0)
-    state32 = H * p.dim * p.dim * 8
+    # complex64 bytes of one state: packed slabs hold d(d+1)/2 elements (state_bytes counts them at 16 B)
+    state32 = int(info.state_bytes) // 2
     per_stage = 11 * state32 / 4
     stage_ms = ms / (args.steps * 4)
     achieved = per_stage / (stage_ms / 1000.0) / 1e9
@@ -636,7 +637,9 @@ def run_mixed(args, cfg: dict) -> None:
                      "traffic": None,
                      "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                      else "fallback 6650 GB/s",
-                     "algorithmic_bytes_per_launch": per_stage, "kernel": "large_kernel<float,8> + large_upterm_kernel",
+                     "algorithmic_bytes_per_launch": per_stage,
+                     "kernel": ("herm_band_kernel<float,8>" if state32 < H * p.dim * p.dim * 8 else "large_kernel<float,8>")
+                     + " + large_upterm_kernel + ado0_kernel",
                      "launch_ms": stage_ms},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": H * p.dim * p.dim * 16 / args.steps,
                 "d2h_bytes_per_step": p.dim * p.dim * 16 + 24,

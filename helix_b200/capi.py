@@ -302,8 +302,8 @@ def rhs_noalloc(problem, rho_device_ptr: int, drho_device_ptr: int, stream_ptr: 
 class Context:
     """One HEOM problem resident on the current CUDA device (wraps hx_ctx).
 
-    For d = 32, 64 the device keeps Hermitian-packed slabs and ``set_state``
-    accepts Hermitian ADOs only; ``full_state=True`` keeps full slabs for
+    For 32 <= d <= 1024 in double precision the device keeps Hermitian-packed
+    slabs and ``set_state`` accepts Hermitian ADOs only; ``full_state=True`` keeps full slabs for
     general states (HX_FLAG_FULL_STATE)."""
 
     def __init__(self, problem, order: int = 4, dt: float | None = None, precision: str = "double",
@@ -320,8 +320,7 @@ class Context:
         self.size = int(self.info.hierarchy_size)
         self.dim = d
         # device slabs hold the upper triangle only (see herm_index)
-        self.hermitian_packed = (prec == PRECISION_DOUBLE and d >= 32 and
-                                 int(self.info.state_bytes) == self.size * (d * (d + 1) // 2) * 16)
+        self.hermitian_packed = (d >= 32 and int(self.info.state_bytes) == self.size * (d * (d + 1) // 2) * 16)
 
     # lifecycle -----------------------------------------------------------
     def close(self) -> None:

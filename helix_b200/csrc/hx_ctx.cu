@@ -163,7 +163,7 @@ hx::FlipArgs flip_args_of(const hx_ctx* c)
 hx::LargeArgs<double> large_args64(const hx_ctx* c)
 {
     hx::LargeArgs<double> a{};
-    a.diag = c->diag_table;
+    a.diag = c->herm ? c->diag_herm : c->diag_table;
     a.vdiag = c->vdiag;
     a.hflip = c->hflip;
     a.gsum = c->gsum;
@@ -180,6 +180,7 @@ hx::LargeArgs<double> large_args64(const hx_ctx* c)
     a.J = c->J;
     a.logd = c->logd;
     a.first_ado = 0;
+    a.herm = c->herm ? 1 : 0;
     return a;
 }
 
@@ -203,19 +204,20 @@ hx::LargeArgs<float> large_args32(const hx_ctx* c)
     a.J = c->J;
     a.logd = c->logd;
     a.first_ado = 1;
+    a.herm = c->herm ? 1 : 0;
     return a;
 }
 
 template <typename R>
 hx::LargeUpArgs<R> large_up_args(const hx_ctx* c, const R* vdiag)
 {
-    return hx::LargeUpArgs<R>{vdiag, c->up_slab, c->bath_off, c->up_slots, c->M, c->J, c->logd};
+    return hx::LargeUpArgs<R>{vdiag, c->up_slab, c->bath_off, c->up_slots, c->M, c->J, c->logd, c->herm ? 1 : 0};
 }
 
 hx::Ado0Args ado0_args(const hx_ctx* c)
 {
-    return hx::Ado0Args{c->diag_table, c->vdiag, c->hflip, c->ent_count, c->ent_slab, c->ent_bath,
-                        c->ent_wc, c->ent_wa, c->M, c->J, c->logd};
+    return hx::Ado0Args{c->herm ? c->diag_herm : c->diag_table, c->vdiag, c->hflip, c->ent_count, c->ent_slab, c->ent_bath,
+                        c->ent_wc, c->ent_wa, c->M, c->J, c->logd, c->herm ? 1 : 0};
 }
 
 // Index of a state buffer of the context: 0 = rho, 1 = ua, 2 = ub.
@@ -495,6 +497,23 @@ HostCsr flip_csr(const double* v, const double* w, int d, int logd)
 // matching buffers (rho32/rho, ua32/ua, ...).
 int read_mixed(hx_ctx* c, const float2* src32, const double2* src64, double* out)
 {
+    if (c->herm) {
+        const size_t P = c->slab_store, count = static_cast<size_t>(c->H) * P;
+        std::vector<float2> tmp(count);
+        std::vector<double2> pk0(P);
+        HX_CUDA_TRY(cudaMemcpyAsync(tmp.data(), src32, count * sizeof(float2), cudaMemcpyDeviceToHost, c->stream));
+        HX_CUDA_TRY(cudaMemcpyAsync(pk0.data(), src64, P * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+        HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        hx::unpack_herm_host(pk0.data(), c->logd, out);
+        parallel_for(c->H - 1, [&](long long k1) {
+            const long long k = k1 + 1;
+            std::vector<double2> w(P);
+            for (size_t i = 0; i < P; ++i) w[i] = make_double2(tmp[k * P + i].x, tmp[k * P + i].y);
+            hx::unpack_herm_host(w.data(), c->logd, out + 2 * static_cast<size_t>(k) * c->slab);
+        });
+        c->counters.d2h_bytes += count * sizeof(float2) + P * sizeof(double2);
+        return HX_OK;
+    }
     const size_t count = static_cast<size_t>(c->H) * c->slab;
     std::vector<float2> tmp(count);
     HX_CUDA_TRY(cudaMemcpyAsync(tmp.data(), src32, count * sizeof(float2), cudaMemcpyDeviceToHost, c->stream));
@@ -670,7 +689,9 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     const bool fused_ok = !c->use_flip && !c->use_large && !c->use_csr && logd >= 5 && logd <= hx::kMaxLogD &&
                           hx::fused_supported(logd, M, J, want_herm ? 1 : 0) &&
                           !(force_generic && force_generic[0] == '1');
-    c->herm = fused_ok && want_herm;
+    // packed band kernels only in double precision: for complex64 their scattered
+    // conjugate gathers cost more than the halved stream saves
+    c->herm = (fused_ok || (c->use_large && !c->mixed)) && want_herm;
     c->slab_store = c->herm ? static_cast<size_t>(hx::herm_elems(logd)) : c->slab;
     const size_t nstate = static_cast<size_t>(H) * c->slab_store;
     if ((rc = dev_alloc(c, &c->vflip, vf.size())) || (rc = upload(c, c->vflip, vf))) return bail(rc);
@@ -690,7 +711,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
             return bail(rc);
     }
     // double-precision state: the whole hierarchy, or only ADO 0 in mixed precision
-    const size_t n64 = c->mixed ? c->slab : nstate;
+    const size_t n64 = c->mixed ? c->slab_store : nstate;
     if (c->mixed && ((rc = dev_alloc(c, &c->rho32, nstate)) || (rc = dev_alloc(c, &c->ua32, nstate)) ||
                      (rc = dev_alloc(c, &c->ub32, nstate))))
         return bail(rc);
@@ -771,7 +792,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
         hx::launch_init_state(c->rho, static_cast<long long>(n64), one, c->stream);
         if (c->mixed) {
             e = cudaMemsetAsync(c->rho32, 0, nstate * sizeof(float2), c->stream);
-            if (e == cudaSuccess) hx::launch_d2f(c->rho, c->rho32, static_cast<long long>(c->slab), c->stream);
+            if (e == cudaSuccess) hx::launch_d2f(c->rho, c->rho32, static_cast<long long>(c->slab_store), c->stream);
             if (e != cudaSuccess) rc = hx::cuda_fail(e, "mixed initial state");
         }
         rc = check_launch("setup kernels");
@@ -814,7 +835,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                     rc = dev_alloc(c, &c->up_slab, static_cast<size_t>(S) * M);
                     if (rc == HX_OK) rc = dev_alloc(c, &c->up_bath, static_cast<size_t>(S) * M);
                     if (rc == HX_OK) {
-                        if (c->mixed) rc = dev_alloc(c, &c->U32, static_cast<size_t>(S) * c->slab);
+                        if (c->mixed) rc = dev_alloc(c, &c->U32, static_cast<size_t>(S) * c->slab_store);
                         else rc = dev_alloc(c, &c->U, static_cast<size_t>(S) * c->slab_store);
                     }
                     if (rc == HX_OK) {
@@ -840,7 +861,8 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                 if ((rc = dev_alloc(c, &c->diag32, c->slab)) || (rc = dev_alloc(c, &c->vdiag32, static_cast<size_t>(J) * d)) ||
                     (rc = dev_alloc(c, &c->hflip32, logd))) {
                 } else {
-                    hx::launch_d2f(c->diag_table, c->diag32, static_cast<long long>(c->slab), c->stream);
+                    hx::launch_d2f(c->herm ? c->diag_herm : c->diag_table, c->diag32,
+                                   static_cast<long long>(c->slab_store), c->stream);
                     hx::launch_vec_d2f(c->vdiag, c->vdiag32, static_cast<long long>(J) * d, c->stream);
                     hx::launch_vec_d2f(c->hflip, c->hflip32, logd, c->stream);
                     rc = check_launch("mixed-precision operators");
@@ -1040,6 +1062,28 @@ int hx_ctx_write_state(hx_ctx* c, const double* in, uint64_t n)
     if (!c || !in) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
     const size_t count = static_cast<size_t>(c->H) * c->slab;
     if (n < 2 * count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "input buffer too small");
+    if (c->mixed && c->herm) {
+        const size_t P = c->slab_store;
+        std::vector<double2> pk(static_cast<size_t>(c->H) * P);
+        std::vector<char> ok(static_cast<size_t>(c->H), 1);
+        parallel_for(c->H, [&](long long k) {
+            ok[k] = pack_herm_host(in + 2 * static_cast<size_t>(k) * c->slab, c->logd, pk.data() + k * P);
+        });
+        for (long long k = 0; k < c->H; ++k)
+            if (!ok[k])
+                return fail(HX_ERR_INVALID_RUNTIME_OPTION,
+                            "ADO " + std::to_string(k) +
+                                " is not Hermitian; this context keeps Hermitian-packed slabs (create it with "
+                                "HX_FLAG_FULL_STATE for general states)");
+        std::vector<float2> tmp(pk.size());
+        for (size_t i = 0; i < pk.size(); ++i)
+            tmp[i] = make_float2(static_cast<float>(pk[i].x), static_cast<float>(pk[i].y));
+        HX_CUDA_TRY(cudaMemcpyAsync(c->rho32, tmp.data(), tmp.size() * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+        HX_CUDA_TRY(cudaMemcpyAsync(c->rho, pk.data(), P * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        c->counters.h2d_bytes += tmp.size() * sizeof(float2) + P * sizeof(double2);
+        HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return HX_OK;
+    }
     if (c->mixed) {
         std::vector<float2> tmp(count);
         for (size_t i = 0; i < count; ++i)
@@ -1132,25 +1176,35 @@ int hx_ctx_load_snapshot(hx_ctx* c, const char* path, uint32_t real_bytes)
     // program (the reference computes (r, c) and (c, r) separately, in single
     // precision by default) is Hermitian to its rounding only: accept up to
     // 1e-5 of each ADO's largest element and store the Hermitian part.
-    const size_t n = static_cast<size_t>(c->H) * c->slab_store;
-    int rc = state_staging(c, n);
-    if (rc != HX_OK) return rc;
-    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    double2* pk = c->state_pinned;
+    const int D = c->d;
     std::vector<char> ok(static_cast<size_t>(c->H), 1);
     parallel_for(c->H, [&](long long k) {
-        ok[k] = pack_herm_host(all.data() + 2 * static_cast<size_t>(k) * c->slab, c->logd, pk + k * c->slab_store,
-                               1e-5, true);
+        double* x = all.data() + 2 * static_cast<size_t>(k) * c->slab;
+        double big2 = 0.0;
+        for (size_t e = 0; e < c->slab; ++e) big2 = std::max(big2, x[2 * e] * x[2 * e] + x[2 * e + 1] * x[2 * e + 1]);
+        const double tol2 = 1e-10 * big2;
+        for (int r = 0; r < D && ok[k]; ++r)
+            for (int q = r; q < D; ++q) {
+                double* a = x + 2 * (static_cast<size_t>(r) * D + q);
+                double* b = x + 2 * (static_cast<size_t>(q) * D + r);
+                const double dr = a[0] - b[0], di = a[1] + b[1];
+                if (dr * dr + di * di > tol2) {
+                    ok[k] = 0;
+                    break;
+                }
+                const double re = 0.5 * (a[0] + b[0]), im = 0.5 * (a[1] - b[1]);
+                a[0] = re;
+                a[1] = im;
+                b[0] = re;
+                b[1] = r == q ? im : -im;
+            }
     });
     for (long long k = 0; k < c->H; ++k)
         if (!ok[k])
             return fail(HX_ERR_INVALID_RUNTIME_OPTION,
                         "ADO " + std::to_string(k) + " of " + path +
                             " is not Hermitian; load it into a context made with HX_FLAG_FULL_STATE");
-    HX_CUDA_TRY(cudaMemcpyAsync(c->rho, pk, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-    c->counters.h2d_bytes += n * sizeof(double2);
-    HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    return HX_OK;
+    return hx_ctx_write_state(c, all.data(), all.size());
 }
 
 int hx_ctx_state_device_ptr(hx_ctx* c, void** ptr)

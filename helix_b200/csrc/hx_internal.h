@@ -188,11 +188,12 @@ struct LargeArgs {
     const double* ent_wc;    // [H][2M]
     const double* ent_wa;    // [H][2M]
     const int32_t* slot;     // [H] slot of a tier L-1 ADO in U, else -1
-    const C2<R>* U;          // [S][d*d]
+    const C2<R>* U;          // [S][d*d], or [S][herm_elems] with herm
     int* error_flag;
     long long H;
     int M, J, logd;
     int first_ado;           // 1 when ADO 0 runs in double precision (ado0_kernel)
+    int herm;                // 1: slabs, diag and U Hermitian-packed (herm_band_kernel)
 };
 template <typename R>
 struct LargeUpArgs {
@@ -200,6 +201,7 @@ struct LargeUpArgs {
     const int32_t* slab;     // [S][M]
     const int32_t* bath_off; // [J+1]
     int S, M, J, logd;
+    int herm;                // 1: slabs and U Hermitian-packed
 };
 struct Ado0Args {
     const double2* diag;     // [d*d]
@@ -211,6 +213,7 @@ struct Ado0Args {
     const double* ent_wc;
     const double* ent_wa;
     int M, J, logd;
+    int herm;                // 1: the slabs (and diag) are Hermitian-packed
 };
 bool large_supported(int logd, int M, int J);
 template <typename R> bool prepare_large(const LargeArgs<R>& a);  // shared-memory limit; call before capture

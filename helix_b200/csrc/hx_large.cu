@@ -215,6 +215,177 @@ __global__ void __launch_bounds__(256, 2)
     }
 }
 
+// Element (r, c) of a Hermitian-packed slab, any r, c.
+template <typename C>
+__device__ __forceinline__ C packed_at(const C* __restrict__ slab, int r, int c, int logd)
+{
+    if (r <= c) return __ldg(slab + herm_index(r, c, logd));
+    const C v = __ldg(slab + herm_index(c, r, logd));
+    C w;
+    w.x = v.x;
+    w.y = -v.y;
+    return w;
+}
+
+// ---------------------------------------------------------------------------
+// Band kernel on Hermitian-packed slabs (layout in hx_internal.h).  A band is
+// G = 2048 / d packed rows: matrix rows s0 .. s0+G-1 and their mirror rows
+// d-1-s0-G+1 .. d-1-s0, so 2G full rows (4096 elements, as a full-slab band)
+// and G (d+1) packed outputs.  The CTA rebuilds those 2G rows in shared
+// memory: the upper parts from the band's own packed rows, the lower parts as
+// conjugates gathered from the other packed rows through L2.  Column flips
+// and the row flips of the low log2 G bits then read shared memory (mirror
+// rows flip with the same local index); flips of higher row bits read the
+// packed slab through L2.  Neighbours, the Horner base, U and the output
+// stream in packed order.  No device-side waits.
+template <typename R, int LOGD>
+__global__ void __launch_bounds__(256, 2)
+    herm_band_kernel(LargeArgs<R> a, const C2<R>* __restrict__ u, const C2<R>* rho, C2<R>* out, double alpha_d,
+                     int base_kind)
+{
+    using C = C2<R>;
+    constexpr int D = 1 << LOGD, T = 256, G = 2048 / D, LOGG = 11 - LOGD;
+    constexpr int NE = G * (D + 1);  // packed elements of a band
+    constexpr int E = (NE + T - 1) / T;
+    constexpr long long P = static_cast<long long>(D / 2) * (D + 1);
+    constexpr int NB = (D / 2) / G;  // bands per slab
+    extern __shared__ __align__(128) unsigned char smem[];
+    C* sx = reinterpret_cast<C*>(smem);                                   // [2G][D] rebuilt rows
+    double* sWc = reinterpret_cast<double*>(smem + 2 * G * D * sizeof(C));  // [2M]
+    double* sWa = sWc + 2 * a.M;                                          // [2M]
+    R* sV = reinterpret_cast<R*>(sWa + 2 * a.M);                          // [J][D]
+    R* sH = sV + a.J * D;                                                 // [LOGD]
+    int* sSlab = reinterpret_cast<int*>(sH + LOGD + 1);                   // [2M]
+    int* sBath = sSlab + 2 * a.M;                                         // [2M]
+
+    const int tid = threadIdx.x;
+    const long long n = a.first_ado + static_cast<long long>(blockIdx.x) / NB;
+    const int s0 = static_cast<int>(blockIdx.x % NB) * G;
+    const int q0 = s0 * (D + 1);  // the band's first packed element
+    const C* un = u + n * P;
+    const int Q = a.ent_count[n];
+    for (int i = tid; i < a.J * D; i += T) sV[i] = a.vdiag[i];
+    if (tid < LOGD) sH[tid] = a.hflip[tid];
+    for (int q = tid; q < Q; q += T) {
+        const long long src = n * 2 * a.M + q;
+        sSlab[q] = a.ent_slab[src];
+        sBath[q] = a.ent_bath[src] & 0xffff;
+        sWc[q] = a.ent_wc[src];
+        sWa[q] = a.ent_wa[src];
+    }
+    const R g = static_cast<R>(a.gsum[n]);
+    const int slot = a.slot ? a.slot[n] : -1;
+    const R alpha = static_cast<R>(alpha_d);
+    // local row of matrix row r of the band
+    auto lrow = [&](int r) { return r < D / 2 ? r - s0 : G + (D - 1 - s0 - r); };
+
+    // ---- rebuild the band's 2G rows: upper parts from the band ...
+    int rc[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        const int i = tid + T * k;
+        int r = 0, c = 0;
+        if (i < NE) {
+            herm_coords(q0 + i, LOGD, r, c);
+            sx[lrow(r) * D + c] = __ldg(un + q0 + i);
+        }
+        rc[k] = (r << 16) | c;
+    }
+    // ... lower parts (c < r) as conjugates of the elements (c, r) of other packed rows
+    for (int t = tid; t < G * (D - 1); t += T) {
+        const int j = t / (D - 1), w = t - j * (D - 1);
+        const int ra = s0 + j;
+        int lr, r, c;
+        if (w < ra) {
+            lr = j;
+            r = ra;
+            c = w;
+        } else {
+            lr = G + j;
+            r = D - 1 - s0 - j;
+            c = w - ra;
+        }
+        const C v = __ldg(un + herm_index(c, r, LOGD));
+        sx[lr * D + c] = mk<R>(v.x, -v.y);
+    }
+    __syncthreads();
+
+    // ---- diagonal table and transverse field
+    C acc[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        const int i = tid + T * k;
+        acc[k] = mk<R>(0, 0);
+        if (i >= NE) continue;
+        const int r = rc[k] >> 16, c = rc[k] & 0xffff, lr = lrow(r);
+        const C x = sx[lr * D + c];
+        const C t = __ldg(a.diag + q0 + i);
+        R hr = 0, hi = 0;
+#pragma unroll
+        for (int b = 0; b < LOGD; ++b) {
+            C rowp;
+            if (b < LOGG) rowp = sx[(lr ^ (1 << b)) * D + c];
+            else rowp = packed_at(un, r ^ (1 << b), c, LOGD);
+            const C colp = sx[lr * D + (c ^ (1 << b))];
+            hr += sH[b] * (rowp.x - colp.x);
+            hi += sH[b] * (rowp.y - colp.y);
+        }
+        const R tr = t.x - g;
+        acc[k].x = tr * x.x - t.y * x.y + hi;
+        acc[k].y = tr * x.y + t.y * x.x - hr;
+    }
+    // ---- neighbour entries, E loads in flight
+    for (int q = 0; q < Q; ++q) {
+        const int j = sBath[q];
+        const R wc = static_cast<R>(sWc[q]), wa = static_cast<R>(sWa[q]);
+        const C* src = u + static_cast<long long>(sSlab[q]) * P + q0 + tid;
+        C y[E];
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+            const int r = rc[k] >> 16, c = rc[k] & 0xffff;
+            const R vr = sV[j * D + r], vc = sV[j * D + c];
+            y[k] = mk<R>(0, 0);
+            if (tid + T * k < NE && ((vr + vc) * wa != R(0) || (vr - vc) * wc != R(0))) y[k] = __ldg(src + T * k);
+        }
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+            const int r = rc[k] >> 16, c = rc[k] & 0xffff;
+            const R vr = sV[j * D + r], vc = sV[j * D + c];
+            const R ar = -(vr + vc) * wa, ai = -(vr - vc) * wc;
+            acc[k].x += ar * y[k].x - ai * y[k].y;
+            acc[k].y += ar * y[k].y + ai * y[k].x;
+        }
+    }
+    // ---- up term of tier L-1, summed by large_upterm_kernel
+    if (slot >= 0) {
+        const C* Un = a.U + static_cast<long long>(slot) * P + q0 + tid;
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+            if (tid + T * k >= NE) continue;
+            const C w = __ldcs(Un + T * k);
+            acc[k].x += w.x;
+            acc[k].y += w.y;
+        }
+    }
+    // ---- Horner epilogue
+    C* on = out + n * P + q0 + tid;
+    const C* rn = rho + n * P + q0 + tid;
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+        if (tid + T * k >= NE) continue;
+        C b;
+        if (base_kind == kBaseSelf) {
+            const int r = rc[k] >> 16, c = rc[k] & 0xffff;
+            b = sx[lrow(r) * D + c];
+        } else if (base_kind == kBaseRho) {
+            b = __ldcs(rn + T * k);
+        } else {
+            b = mk<R>(0, 0);
+        }
+        __stcs(on + T * k, mk<R>(b.x + alpha * acc[k].x, b.y + alpha * acc[k].y));
+    }
+}
+
 // Up term of tier L-1 in the working precision, tile-major so the top-tier
 // data of the resident tiles stays in L2 (as upterm_kernel, hx_upterm.cu).
 constexpr int kUpWarps = 8, kUpSlots = 4, kUpTile = 32;
@@ -225,10 +396,18 @@ __global__ void __launch_bounds__(kUpWarps * 32)
 {
     using C = C2<R>;
     const int D = 1 << a.logd;
-    const long long D2 = static_cast<long long>(D) * D;
+    // elements per stored slab: d^2, or the packed upper triangle
+    const long long D2 = a.herm ? herm_elems(a.logd) : static_cast<long long>(D) * D;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long e = static_cast<long long>(blockIdx.y) * kUpTile + lane;
-    const int r = static_cast<int>(e >> a.logd), c = static_cast<int>(e & (D - 1));
+    if (e >= D2) return;
+    int r, c;
+    if (a.herm) {
+        herm_coords(static_cast<int>(e), a.logd, r, c);
+    } else {
+        r = static_cast<int>(e >> a.logd);
+        c = static_cast<int>(e & (D - 1));
+    }
     const C* ue = u + e;
     const int s0 = (blockIdx.x * kUpWarps + warp) * kUpSlots;
     for (int s = s0; s < s0 + kUpSlots && s < a.S; ++s) {
@@ -260,16 +439,28 @@ __global__ void __launch_bounds__(256)
                 double2* out0, float2* out32, double alpha, int base_kind)
 {
     const int D = 1 << a.logd;
-    const long long D2 = static_cast<long long>(D) * D;
+    const long long D2 = a.herm ? herm_elems(a.logd) : static_cast<long long>(D) * D;
     const long long ge = blockIdx.x * 256ll + threadIdx.x;
     if (ge >= D2) return;
-    const int r = static_cast<int>(ge >> a.logd), c = static_cast<int>(ge & (D - 1));
+    int r, c;
+    if (a.herm) {
+        herm_coords(static_cast<int>(ge), a.logd, r, c);
+    } else {
+        r = static_cast<int>(ge >> a.logd);
+        c = static_cast<int>(ge & (D - 1));
+    }
     const double2 x = u0[ge];
     const double2 t = a.diag[ge];
     double hr = 0.0, hi = 0.0;
     for (int i = 0; i < a.logd; ++i) {
-        const double2 p = u0[ge ^ (static_cast<long long>(D) << i)];
-        const double2 q = u0[ge ^ (1ll << i)];
+        double2 p, q;
+        if (a.herm) {
+            p = packed_at(u0, r ^ (1 << i), c, a.logd);
+            q = packed_at(u0, r, c ^ (1 << i), a.logd);
+        } else {
+            p = u0[ge ^ (static_cast<long long>(D) << i)];
+            q = u0[ge ^ (1ll << i)];
+        }
         hr += a.hflip[i] * (p.x - q.x);
         hi += a.hflip[i] * (p.y - q.y);
     }
@@ -327,13 +518,18 @@ bool launch_t(const LargeArgs<R>& a, const C2<R>* u, const C2<R>* rho, C2<R>* ou
     cudaGetDevice(&dev);
     if (dev < 64 && configured[dev] < smem) {
         if (cudaFuncSetAttribute(large_kernel<R, LOGD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)) != cudaSuccess ||
+            cudaFuncSetAttribute(herm_band_kernel<R, LOGD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)) != cudaSuccess)
             return false;
         configured[dev] = smem;
     }
     if (!launch) return true;
+    // bands per slab: d^2 / 4096 full-slab bands, or (d / 2) / (2048 / d) = d^2 / 4096 packed bands
     const long long nb = (a.H - a.first_ado) * ((1ll << (2 * LOGD)) / 4096);
-    if (nb > 0) large_kernel<R, LOGD><<<static_cast<unsigned>(nb), 256, smem, s>>>(a, u, rho, out, alpha, base);
+    if (nb <= 0) return true;
+    if (a.herm) herm_band_kernel<R, LOGD><<<static_cast<unsigned>(nb), 256, smem, s>>>(a, u, rho, out, alpha, base);
+    else large_kernel<R, LOGD><<<static_cast<unsigned>(nb), 256, smem, s>>>(a, u, rho, out, alpha, base);
     return true;
 }
 
@@ -377,9 +573,9 @@ template <typename R>
 void launch_large_upterm(const LargeUpArgs<R>& a, const C2<R>* u, C2<R>* U, cudaStream_t s)
 {
     if (a.S <= 0) return;
-    const long long D2 = 1ll << (2 * a.logd);
+    const long long D2 = a.herm ? herm_elems(a.logd) : 1ll << (2 * a.logd);
     const int per = kUpWarps * kUpSlots;
-    dim3 grid((a.S + per - 1) / per, static_cast<unsigned>(D2 / kUpTile));
+    dim3 grid((a.S + per - 1) / per, static_cast<unsigned>((D2 + kUpTile - 1) / kUpTile));
     large_upterm_kernel<R><<<grid, kUpWarps * 32, 0, s>>>(a, u, U);
 }
 
@@ -395,7 +591,7 @@ template void launch_large_upterm<float>(const LargeUpArgs<float>&, const float2
 void launch_ado0(const Ado0Args& a, const double2* u0, const float2* u, const double2* rho0, double2* out0,
                  float2* out32, double alpha, int base_kind, cudaStream_t s)
 {
-    const long long D2 = 1ll << (2 * a.logd);
+    const long long D2 = a.herm ? herm_elems(a.logd) : 1ll << (2 * a.logd);
     ado0_kernel<<<static_cast<unsigned>((D2 + 255) / 256), 256, 0, s>>>(a, u0, u, rho0, out0, out32, alpha, base_kind);
 }
 

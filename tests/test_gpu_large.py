@@ -19,20 +19,30 @@ def _trace_distance(a, b):
     return 0.5 * float(np.sum(np.abs(np.linalg.eigvalsh(0.5 * (m + m.conj().T)))))
 
 
-def test_band_kernel_fp64_rhs_and_steps_d128():
+def _hermitian(x):
+    return 0.5 * (x + np.conj(np.transpose(x, (0, 2, 1))))
+
+
+@pytest.mark.parametrize("state", ["hermitian", "general"])
+def test_band_kernel_fp64_rhs_and_steps_d128(state):
+    """Hermitian states on the default packed band kernel, random complex
+    states on full slabs (full_state=True)."""
     p = S.spin_glass(7, seed=31, depth=2, K=1, h=0.8, dt=0.01)
     o = O.Oracle(p)
     rng = np.random.default_rng(3)
     x = (rng.standard_normal((o.size, p.dim, p.dim)) + 1j * rng.standard_normal((o.size, p.dim, p.dim))) * 0.1
     x[0] = 0.5 * (x[0] + x[0].conj().T)
-    with capi.Context(p) as ctx:
+    if state == "hermitian":
+        x = _hermitian(x)
+    with capi.Context(p, full_state=state == "general") as ctx:
+        assert ctx.hermitian_packed == (state == "hermitian")
         ctx.set_state(x)
         r = ctx.rhs()
         ref = o.rhs(x)
         assert np.max(np.abs(r - ref)) < 1e-12 * max(1.0, np.max(np.abs(ref)))
     rho_ref, en_ref = o.run(6, trace=True)
     o.close()
-    with capi.Context(p) as ctx:
+    with capi.Context(p, full_state=state == "general") as ctx:
         rho, en = ctx.step_trace(6)
     assert np.max(np.abs(rho - rho_ref)) < TOL
     assert np.max(np.abs(en - en_ref)) < TOL
@@ -75,14 +85,18 @@ def test_mixed_precision_tracks_fp64_within_trace_distance():
     assert np.max(np.abs(r64[7] - ro[7])) < TOL
 
 
-def test_mixed_precision_state_roundtrip_and_rhs():
+@pytest.mark.parametrize("state", ["hermitian", "general"])
+def test_mixed_precision_state_roundtrip_and_rhs(state):
     p = S.spin_glass(7, seed=2, depth=2, K=1, h=0.5, dt=0.005)
     o = O.Oracle(p)
     rng = np.random.default_rng(9)
     x = (rng.standard_normal((o.size, p.dim, p.dim)) + 1j * rng.standard_normal((o.size, p.dim, p.dim))) * 0.05
+    if state == "hermitian":
+        x = _hermitian(x)
     ref = o.rhs(x)
     o.close()
-    with capi.Context(p, precision="mixed") as cm:
+    with capi.Context(p, precision="mixed", full_state=state == "general") as cm:
+        assert not cm.hermitian_packed  # the complex64 band kernels keep full slabs
         cm.set_state(x)
         back = cm.state()
         assert np.max(np.abs(back[0] - x[0])) == 0.0  # ADO 0 is stored in double precision
@@ -99,3 +113,18 @@ def test_mixed_precision_rejects_unsupported_shapes():
     with pytest.raises(capi.HxError) as e:
         capi.Context(S.spin_glass(7, seed=1, depth=1), precision="mixed")  # max_depth 2
     assert e.value.status == "UnsupportedPrecision"
+
+
+def test_packed_band_kernels_d256_and_d512_match_oracle():
+    """Packed band kernels with several bands per slab and the L2 row-flip
+    gathers (d = 256: 16 bands of 8 packed rows; d = 512: 64 bands of 4)."""
+    for n in (8, 9):
+        p = S.spin_glass(n, seed=70 + n, depth=1, K=1, h=0.6, dt=0.005)
+        o = O.Oracle(p)
+        rho_ref, en_ref = o.run(3, trace=True)
+        o.close()
+        with capi.Context(p) as ctx:
+            assert ctx.hermitian_packed
+            rho, en = ctx.step_trace(3)
+        assert np.max(np.abs(rho - rho_ref)) < TOL
+        assert np.max(np.abs(en - en_ref)) < TOL
