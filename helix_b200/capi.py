@@ -25,7 +25,7 @@ STATUS_NAMES = {
 }
 PRECISION_DOUBLE = 1
 PRECISION_MIXED = 2  # complex64 hierarchy, ADO 0 (rho_0) in double precision
-FLAG_FULL_STATE = 1  # keep full d x d slabs on the device (FP64 contexts with 32 <= d <= 1024 default to Hermitian-packed)
+FLAG_FULL_STATE = 1  # keep full d x d slabs on the device (contexts with 32 <= d <= 1024 default to Hermitian-packed)
 
 # Every exported symbol of include/helix_b200.h
 EXPORTS = [
@@ -225,7 +225,7 @@ def seeded_couplings(n: int, seed: int) -> np.ndarray:
 
 def herm_index(r: int, c: int, d: int) -> int:
     """Position of element (r, c), r <= c, in a Hermitian-packed slab of a
-    d x d matrix (the device layout of FP64 contexts with 32 <= d <= 1024): d/2 packed rows
+    d x d matrix (the device layout of contexts with 32 <= d <= 1024): d/2 packed rows
     of d + 1 elements, packed row s = row s from the diagonal on, then row
     d-1-s from the diagonal on."""
     return r * (d + 1) + (c - r) if r < d // 2 else (d - 1 - r) * (d + 1) + c + 1
@@ -302,8 +302,8 @@ def rhs_noalloc(problem, rho_device_ptr: int, drho_device_ptr: int, stream_ptr: 
 class Context:
     """One HEOM problem resident on the current CUDA device (wraps hx_ctx).
 
-    For 32 <= d <= 1024 in double precision the device keeps Hermitian-packed
-    slabs and ``set_state`` accepts Hermitian ADOs only; ``full_state=True`` keeps full slabs for
+    For 32 <= d <= 1024 the device keeps Hermitian-packed slabs and
+    ``set_state`` accepts Hermitian ADOs only; ``full_state=True`` keeps full slabs for
     general states (HX_FLAG_FULL_STATE)."""
 
     def __init__(self, problem, order: int = 4, dt: float | None = None, precision: str = "double",

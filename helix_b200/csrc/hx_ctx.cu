@@ -689,9 +689,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     const bool fused_ok = !c->use_flip && !c->use_large && !c->use_csr && logd >= 5 && logd <= hx::kMaxLogD &&
                           hx::fused_supported(logd, M, J, want_herm ? 1 : 0) &&
                           !(force_generic && force_generic[0] == '1');
-    // packed band kernels only in double precision: for complex64 their scattered
-    // conjugate gathers cost more than the halved stream saves
-    c->herm = (fused_ok || (c->use_large && !c->mixed)) && want_herm;
+    c->herm = (fused_ok || c->use_large) && want_herm;
     c->slab_store = c->herm ? static_cast<size_t>(hx::herm_elems(logd)) : c->slab;
     const size_t nstate = static_cast<size_t>(H) * c->slab_store;
     if ((rc = dev_alloc(c, &c->vflip, vf.size())) || (rc = upload(c, c->vflip, vf))) return bail(rc);

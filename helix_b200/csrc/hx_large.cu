@@ -215,15 +215,16 @@ __global__ void __launch_bounds__(256, 2)
     }
 }
 
-// Element (r, c) of a Hermitian-packed slab, any r, c.
+// Element (r, c) of a Hermitian-packed slab, any r, c (one load, no branch
+// around it, so several lookups can be in flight at once).
 template <typename C>
 __device__ __forceinline__ C packed_at(const C* __restrict__ slab, int r, int c, int logd)
 {
-    if (r <= c) return __ldg(slab + herm_index(r, c, logd));
-    const C v = __ldg(slab + herm_index(c, r, logd));
+    const bool lower = r > c;
+    const C v = __ldg(slab + herm_index(lower ? c : r, lower ? r : c, logd));
     C w;
     w.x = v.x;
-    w.y = -v.y;
+    w.y = lower ? -v.y : v.y;
     return w;
 }
 
@@ -292,6 +293,7 @@ __global__ void __launch_bounds__(256, 2)
         rc[k] = (r << 16) | c;
     }
     // ... lower parts (c < r) as conjugates of the elements (c, r) of other packed rows
+#pragma unroll 4
     for (int t = tid; t < G * (D - 1); t += T) {
         const int j = t / (D - 1), w = t - j * (D - 1);
         const int ra = s0 + j;

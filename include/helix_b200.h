@@ -105,8 +105,8 @@ typedef struct hx_problem {
 
 /* Every ADO of this hierarchy stays Hermitian (H and the V_j are Hermitian
  * and every term of the right-hand side maps Hermitian matrices to Hermitian
- * matrices), so for d = 32 ... 1024 in double precision the device state
- * keeps the upper triangle of each slab only (d(d+1)/2 elements instead of
+ * matrices), so for d = 32 ... 1024 the device state (complex64 in mixed
+ * precision) keeps the upper triangle of each slab only (d(d+1)/2 elements instead of
  * d^2), which halves the memory traffic of a step.  The C ABI still reads and writes full d x d
  * slabs; hx_ctx_write_state then rejects non-Hermitian ADOs.  This flag keeps
  * full slabs on the device, for general (non-Hermitian) states. */
@@ -240,7 +240,7 @@ int hx_write_energy_trace(const char* path, const double* times, const double* e
 /* Device pointer of the state (hierarchy_size * d * d double2), for callers
  * that fill or read it on the device.  In mixed precision this is the
  * double-precision slab of ADO 0 only (d * d double2).  With Hermitian-packed
- * slabs (32 <= d <= 1024 in double precision, without HX_FLAG_FULL_STATE) each slab holds d(d+1)/2
+ * slabs (32 <= d <= 1024, without HX_FLAG_FULL_STATE) each slab holds d(d+1)/2
  * double2: element (r, c), r <= c, at r*(d+1) + c - r when r < d/2, else at
  * (d-1-r)*(d+1) + c + 1. */
 int hx_ctx_state_device_ptr(hx_ctx* ctx, void** ptr);

@@ -96,7 +96,7 @@ def test_mixed_precision_state_roundtrip_and_rhs(state):
     ref = o.rhs(x)
     o.close()
     with capi.Context(p, precision="mixed", full_state=state == "general") as cm:
-        assert not cm.hermitian_packed  # the complex64 band kernels keep full slabs
+        assert cm.hermitian_packed == (state == "hermitian")
         cm.set_state(x)
         back = cm.state()
         assert np.max(np.abs(back[0] - x[0])) == 0.0  # ADO 0 is stored in double precision
