@@ -239,13 +239,18 @@ __device__ __forceinline__ C packed_at(const C* __restrict__ slab, int r, int c,
 // rows flip with the same local index); flips of higher row bits read the
 // packed slab through L2.  Neighbours, the Horner base, U and the output
 // stream in packed order.  No device-side waits.
+// Threads per band: complex64 bands hide their L2 gathers with 512 threads
+// (5 elements each); double-precision ones need the registers of 256 (9 each).
+template <typename R> struct BandThreads { static constexpr int T = 256; };
+template <> struct BandThreads<float> { static constexpr int T = 512; };
+
 template <typename R, int LOGD>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(BandThreads<R>::T, 2)
     herm_band_kernel(LargeArgs<R> a, const C2<R>* __restrict__ u, const C2<R>* rho, C2<R>* out, double alpha_d,
                      int base_kind)
 {
     using C = C2<R>;
-    constexpr int D = 1 << LOGD, T = 256, G = 2048 / D, LOGG = 11 - LOGD;
+    constexpr int D = 1 << LOGD, T = BandThreads<R>::T, G = 2048 / D, LOGG = 11 - LOGD;
     constexpr int NE = G * (D + 1);  // packed elements of a band
     constexpr int E = (NE + T - 1) / T;
     constexpr long long P = static_cast<long long>(D / 2) * (D + 1);
@@ -530,7 +535,8 @@ bool launch_t(const LargeArgs<R>& a, const C2<R>* u, const C2<R>* rho, C2<R>* ou
     // bands per slab: d^2 / 4096 full-slab bands, or (d / 2) / (2048 / d) = d^2 / 4096 packed bands
     const long long nb = (a.H - a.first_ado) * ((1ll << (2 * LOGD)) / 4096);
     if (nb <= 0) return true;
-    if (a.herm) herm_band_kernel<R, LOGD><<<static_cast<unsigned>(nb), 256, smem, s>>>(a, u, rho, out, alpha, base);
+    if (a.herm)
+        herm_band_kernel<R, LOGD><<<static_cast<unsigned>(nb), BandThreads<R>::T, smem, s>>>(a, u, rho, out, alpha, base);
     else large_kernel<R, LOGD><<<static_cast<unsigned>(nb), 256, smem, s>>>(a, u, rho, out, alpha, base);
     return true;
 }
