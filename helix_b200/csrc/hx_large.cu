@@ -240,8 +240,8 @@ __device__ __forceinline__ C packed_at(const C* __restrict__ slab, int r, int c,
 // packed slab through L2.  Neighbours, the Horner base, U and the output
 // stream in packed order.  No device-side waits.
 // Threads per band: complex64 bands hide their L2 gathers with 512 threads
-// (5 elements each); double-precision ones need the registers of 256 (9 each).
-template <typename R> struct BandThreads { static constexpr int T = 256; };
+// (5 elements each); double-precision ones need more registers: 384 (6 each).
+template <typename R> struct BandThreads { static constexpr int T = 384; };
 template <> struct BandThreads<float> { static constexpr int T = 512; };
 
 template <typename R, int LOGD>
