@@ -700,7 +700,7 @@ def run_closure(args, cfg: dict) -> None:
     t_train = time.perf_counter() - t0
     info = cl.info()
 
-    # held-out seeds: plain L=5 (judge), plain L=2, L=2 + closure; device-timed runs
+    # held-out seeds: plain L=5 (the reference solution), plain L=2, L=2 + closure; device-timed runs
     stream = torch.cuda.Stream()
 
     def run(p, closure=None, timed=True):

@@ -7,7 +7,7 @@ Outputs (tests/golden/):
 * ``reference_tables.json`` — hierarchy rows/edges from the reference's own
   ``initialize_detail.h`` builders (compiled from source by
   ``oracle/build.py``): full tables for small shapes, SHA-256 digests for the
-  large ones (C1, C2, C3, C5 truncation and judge shapes).
+  large ones (C1, C2, C3, C5 truncated and deep-reference shapes).
 * ``reference_psd.json`` — poles/residues from the reference's
   ``getPsdPoleResidue`` for K = 1..8.
 * ``reference_legacy_h.json`` — legacy diagonal Hamiltonian entries from the
