@@ -46,6 +46,7 @@ CONFIGS = {
     # L=5 FP64 runs (dt=0.01, 1000 steps), tested on 16 held-out seeds against plain L=5
     "c5": dict(n=5, K=2, h=1.0, dt=0.01, closure=True, coarse_depth=2, fine_depth=5, train_seeds=16,
                test_seeds=16, traj_steps=1000, every=50, hidden=128, iters=3000, mlp_batch=8192, lr=3e-3,
+               time_seeds=4, time_steps=250,
                workload="spin_glass_d32_K2_L2_plus_mlp_closure_vs_L5"),
     # batched disorder average: 512 seeded instances, N in {3,4,5}, L in {2,3,4}, K=2, dt=0.01
     "c4": dict(batch=True, count=512, seed=2026, dt=0.01, workload="disorder_batch_512_N3-5_L2-4_K2_fp64"),
@@ -96,29 +97,45 @@ class ClockSampler:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    INTERVAL_MS = 50
+
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
         self.thread = None
+        self.t0 = None
 
     def start(self):
+        """Start sampling and return once the first sample has arrived (or
+        after 5 s), so that the timed region that follows is covered."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.INTERVAL_MS)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
+            return
+        deadline = time.monotonic() + 5.0
+        while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.t0 = time.monotonic()
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def stop(self) -> dict:
+        """Stop after one more sample has arrived; keep the samples taken
+        between start() returning and that sample."""
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t1 = time.monotonic()
+        deadline = t1 + 2.0
+        while time.monotonic() < deadline and self.proc.poll() is None and not any(t >= t1 for t, _ in self.lines):
+            time.sleep(0.005)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -128,7 +145,12 @@ class ClockSampler:
             self.thread.join(timeout=2)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0 = self.t0 if self.t0 is not None else 0.0
+        after = [t for t, _ in self.lines if t >= t1]
+        t_end = after[0] if after else float("inf")
+        for t, ln in self.lines:
+            if t < t0 or t > t_end:
+                continue
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -142,6 +164,50 @@ class ClockSampler:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+class L2Flush:
+    """Device timing of single steps with L2 flushed in between: for a state
+    smaller than L2 every timed step starts from a cold L2 (the flush buffer,
+    twice the L2 size, is written on the same stream between the timed
+    events)."""
+
+    def __init__(self, stream, device: int):
+        import torch
+
+        self.torch = torch
+        self.stream = stream
+        l2 = int(getattr(torch.cuda.get_device_properties(device), "L2_cache_size", 0)) or 126 * 2**20
+        self.l2_bytes = l2
+        self.buf = torch.empty(2 * l2, dtype=torch.uint8, device=f"cuda:{device}")
+
+    def flush(self):
+        with self.torch.cuda.stream(self.stream):
+            self.buf.zero_()
+
+    def time_steps(self, step_one, steps: int) -> float:
+        """Sum of the device times of `steps` calls of step_one() (ms)."""
+        torch = self.torch
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in ev:
+            self.flush()
+            a.record(self.stream)
+            step_one()
+            b.record(self.stream)
+        torch.cuda.synchronize()
+        return float(sum(a.elapsed_time(b) for a, b in ev))
+
+
+def stage_kernels_label(cfg: dict, p, packed: bool, per_stage: int) -> str:
+    """The kernels one stage of this context launches."""
+    logd = p.dim.bit_length() - 1
+    if cfg.get("legacy"):
+        return "comm_kernel + combine_kernel per stage (spin-flip coupling path)"
+    if p.dim in (32, 64):
+        k = f"herm_kernel<{logd}>" if packed else f"fused_kernel<{logd}>"
+        return k + (" + upterm_kernel" if per_stage == 2 else "") + " per stage" + \
+            (" (Hermitian-packed slabs)" if packed else "")
+    return "stage_kernel per stage (generic path)"
 
 
 def cpu_model() -> str:
@@ -263,6 +329,9 @@ def run_ours(args, cfg: dict) -> None:
             dist.barrier()
 
     # ---- device-resident throughput (value) --------------------------------
+    # a state smaller than L2 is timed step by step with L2 flushed in between
+    flusher = L2Flush(stream, local)
+    small = state_bytes < flusher.l2_bytes
     for _ in range(args.warmup):
         ctx.step(1)
     ctx.sync()
@@ -271,15 +340,19 @@ def run_ours(args, cfg: dict) -> None:
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    ctx.step(args.steps)
-    ev1.record(stream)
-    ctx.sync()
-    torch.cuda.synchronize()
+    if small:
+        ms = flusher.time_steps(lambda: ctx.step(1), args.steps)
+    else:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        ctx.step(args.steps)
+        ev1.record(stream)
+        ctx.sync()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
+    del flusher
     c1 = ctx.counters()
     launches = int(c1.kernel_launches - c0.kernel_launches)
     if world > 1:
@@ -348,16 +421,18 @@ def run_ours(args, cfg: dict) -> None:
                        "depth_L": p.max_depth - 1,
                        "dt": p.dt, "integrator": "RK4 (4-term Taylor, Horner form)",
                        "parallelism": "replicas" if world > 1 else "single",
-                       "l2": f"inputs larger than L2 (state {state_bytes / 1e9:.3f} GB)"},
+                       "l2": (f"L2 flushed before every timed step (state {state_bytes / 1e6:.1f} MB fits in L2; "
+                              "steps timed one by one with CUDA events, flush outside the events)") if small
+                       else f"inputs larger than L2 (state {state_bytes / 1e9:.3f} GB)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
                          "algorithmic_bytes_per_launch": per_launch_bytes,
-                         "kernel": (f"{kernel}<{p.dim.bit_length() - 1}> + upterm_kernel per stage"
-                                    + (" (Hermitian-packed slabs)" if packed else "")),
-                         "traffic_source": f"dram bytes of one stage from profiles/{kernel}_{args.config}_ncu.txt "
-                                           f"+ profiles/upterm_kernel_{args.config}_ncu.txt",
+                         "kernel": stage_kernels_label(cfg, p, packed, info_kernels_per_stage(ctx)),
+                         "traffic_source": (f"dram bytes of one stage from profiles/{kernel}_{args.config}_ncu.txt "
+                                            f"+ profiles/upterm_kernel_{args.config}_ncu.txt") if traffic is not None
+                         else "no ncu summary of this workload under profiles/",
                          "launch_ms": launch_ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": slab_elems * 16 + 24,
@@ -700,58 +775,73 @@ def run_closure(args, cfg: dict) -> None:
     t_train = time.perf_counter() - t0
     info = cl.info()
 
-    # held-out seeds: plain L=5 (the reference solution), plain L=2, L=2 + closure; device-timed runs
+    # held-out seeds: plain L=5 (the reference solution), plain L=2 and L=2 +
+    # closure over the full trajectory (errors, untimed); then the step rate of
+    # each form on the first seeds, timed step by step with L2 flushed in between
     stream = torch.cuda.Stream()
+    flusher = L2Flush(stream, local)
 
-    def run(p, closure=None, timed=True):
-        ctx = capi.Context(p)
-        ctx.set_stream(stream.cuda_stream)
-        if closure is not None:
-            closure.attach(ctx)
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        k0 = ctx.counters().kernel_launches
-        ev0.record(stream)
-        rho, _ = ctx.step_trace(steps, rho0=True, energy=False)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        H = ctx.size
-        launches[0] += int(ctx.counters().kernel_launches - k0) if closure is not None else 0
-        ctx.close()
-        return rho, ev0.elapsed_time(ev1), H
+    def trajectory(p, closure=None):
+        with capi.Context(p) as ctx:
+            if closure is not None:
+                closure.attach(ctx)
+            rho, _ = ctx.step_trace(steps, rho0=True, energy=False)
+            return rho, ctx.size
 
-    e_plain, e_closed, ms_fine, ms_closed, ms_plain = [], [], 0.0, 0.0, 0.0
-    launches = [0]
-    clocks = ClockSampler(local)
-    clocks.start()
+    def step_rate(p, closure=None):
+        with capi.Context(p) as ctx:
+            ctx.set_stream(stream.cuda_stream)
+            if closure is not None:
+                closure.attach(ctx)
+            for _ in range(args.warmup):
+                ctx.step(1)
+            ctx.sync()
+            k0 = ctx.counters().kernel_launches
+            ms = flusher.time_steps(lambda: ctx.step(1), time_steps)
+            return ms, int(ctx.counters().kernel_launches - k0)
+
+    e_plain, e_closed = [], []
     for s in test_seeds:
-        ref, mf, H_fine = run(problem(s, cfg["fine_depth"]))
-        plain, mp, _ = run(problem(s, cfg["coarse_depth"]))
-        closed, mc, H_coarse = run(problem(s, cfg["coarse_depth"]), cl)
-        ms_fine += mf
-        ms_plain += mp
-        ms_closed += mc
+        ref, H_fine = trajectory(problem(s, cfg["fine_depth"]))
+        plain, _ = trajectory(problem(s, cfg["coarse_depth"]))
+        closed, H_coarse = trajectory(problem(s, cfg["coarse_depth"]), cl)
         e_plain.append(max(td(plain[t], ref[t]) for t in range(0, steps, 10)))
         e_closed.append(max(td(closed[t], ref[t]) for t in range(0, steps, 10)))
+    time_seeds = test_seeds[:cfg["time_seeds"]]
+    time_steps = cfg["time_steps"]
+    ms_fine = ms_plain = ms_closed = 0.0
+    launches = 0
+    clocks = ClockSampler(local)
+    clocks.start()
+    for s in time_seeds:
+        ms_fine += step_rate(problem(s, cfg["fine_depth"]))[0]
+        ms_plain += step_rate(problem(s, cfg["coarse_depth"]))[0]
+        mc, lc = step_rate(problem(s, cfg["coarse_depth"]), cl)
+        ms_closed += mc
+        launches += lc
     clk = clocks.stop()
     cl.close()
+    del flusher
     nt = len(test_seeds)
-    value = H_coarse * steps * nt / (ms_closed / 1000.0)
+    timed = len(time_seeds) * time_steps
+    value = H_coarse * timed / (ms_closed / 1000.0)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps * nt, "warmup": 0,
-        "ms_per_step": ms_closed / (steps * nt), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": timed, "warmup": args.warmup,
+        "ms_per_step": ms_closed / timed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 hierarchy, bf16 MLP (f32 accumulation)", "data": "synthetic",
         "config": {"workload": cfg["workload"], "ados_coarse": H_coarse, "ados_fine": H_fine, "dim": 1 << n,
                    "modes": 3 * n, "coarse_depth_L": cfg["coarse_depth"], "fine_depth_L": cfg["fine_depth"],
                    "dt": dt, "train_seeds": len(train_seeds), "test_seeds": nt, "trajectory_steps": steps,
-                   "snapshot_every": every,
+                   "snapshot_every": every, "timed": f"{time_steps} steps on each of {len(time_seeds)} held-out "
+                                                  "seeds per form, after the warm-up",
+                   "l2": "L2 flushed before every timed step (steps timed one by one with CUDA events)",
                    "mlp": f"features of (mode, n_k, r, c) {3 * n + 3 + cfg['coarse_depth'] + 1}-{cfg['hidden']}-"
                    f"{cfg['hidden']}-2 GELU -> complex coefficient of rho_n(r, c); table of "
                    f"{3 * n * (cfg['coarse_depth'] + 1) * (1 << n) ** 2} coefficients, elementwise closure kernel",
                    "parallelism": "single"},
-        "closure": {"simulated_steps_per_s": steps * nt / (ms_closed / 1000.0),
-                    "plain_fine_steps_per_s": steps * nt / (ms_fine / 1000.0),
-                    "plain_coarse_steps_per_s": steps * nt / (ms_plain / 1000.0),
+        "closure": {"simulated_steps_per_s": timed / (ms_closed / 1000.0),
+                    "plain_fine_steps_per_s": timed / (ms_fine / 1000.0),
+                    "plain_coarse_steps_per_s": timed / (ms_plain / 1000.0),
                     "speedup_vs_plain_fine": ms_fine / ms_closed,
                     "trace_distance_vs_fine": {"closure_max": max(e_closed), "closure_mean": float(np.mean(e_closed)),
                                                "truncated_max": max(e_plain), "truncated_mean": float(np.mean(e_plain))},
@@ -759,7 +849,7 @@ def run_closure(args, cfg: dict) -> None:
                     "train": {"snapshots": info["snapshots"], "data_s": t_data, "train_s": t_train,
                               "iters": cfg["iters"], "batch": cfg["mlp_batch"], "loss_first": float(loss[:20].mean()),
                               "loss_last": float(loss[-100:].mean())}},
-        "gpu_launches": launches[0],
+        "gpu_launches": launches,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
