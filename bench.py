@@ -198,12 +198,17 @@ class L2Flush:
         return float(sum(a.elapsed_time(b) for a, b in ev))
 
 
-def stage_kernels_label(cfg: dict, p, packed: bool, per_stage: int) -> str:
-    """The kernels one stage of this context launches."""
+def stage_kernels_label(ctx, p, packed: bool, per_stage: int) -> str:
+    """The kernels one stage of this context launches (from its stage path)."""
     logd = p.dim.bit_length() - 1
-    if cfg.get("legacy"):
+    path = ctx.stage_path
+    if path == "flip":
         return "comm_kernel + combine_kernel per stage (spin-flip coupling path)"
-    if p.dim in (32, 64):
+    if path == "csr":
+        return "csr_comm_kernel + csr_combine_kernel per stage (general sparse operators)"
+    if path == "band":
+        return "band kernels per stage" + (" (Hermitian-packed slabs)" if packed else "")
+    if path == "fused":
         k = f"herm_kernel<{logd}>" if packed else f"fused_kernel<{logd}>"
         return k + (" + upterm_kernel" if per_stage == 2 else "") + " per stage" + \
             (" (Hermitian-packed slabs)" if packed else "")
@@ -429,7 +434,7 @@ def run_ours(args, cfg: dict) -> None:
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
                          "algorithmic_bytes_per_launch": per_launch_bytes,
-                         "kernel": stage_kernels_label(cfg, p, packed, info_kernels_per_stage(ctx)),
+                         "kernel": stage_kernels_label(ctx, p, packed, info_kernels_per_stage(ctx)),
                          "traffic_source": (f"dram bytes of one stage from profiles/{kernel}_{args.config}_ncu.txt "
                                             f"+ profiles/upterm_kernel_{args.config}_ncu.txt") if traffic is not None
                          else "no ncu summary of this workload under profiles/",

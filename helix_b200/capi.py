@@ -84,7 +84,11 @@ def _csr_struct(ptr, col, val, keep):
 class Info(C.Structure):
     _fields_ = [("dim", C.c_uint32), ("modes", C.c_uint32), ("hierarchy_size", C.c_uint64),
                 ("state_bytes", C.c_uint64), ("device_bytes", C.c_uint64), ("steps_done", C.c_uint64),
-                ("time", C.c_double), ("kernels_per_step", C.c_uint32)]
+                ("time", C.c_double), ("kernels_per_step", C.c_uint32), ("stage_path", C.c_uint32)]
+
+
+# hx_info.stage_path (HX_PATH_*)
+STAGE_PATHS = {0: "generic", 1: "fused", 2: "band", 3: "flip", 4: "csr"}
 
 
 class Counters(C.Structure):
@@ -256,7 +260,8 @@ def _problem_struct(problem, order: int = 4, dt: float | None = None, precision:
     keep += [hd, hf]
     baths = (_Bath * len(problem.baths))()
     for j, b in enumerate(problem.baths):
-        if b.v_csr is not None:
+        # the diagonal (+ flip weights) form when the bath gives one, else its CSR form
+        if b.v_diag is None and b.v_csr is not None:
             baths[j] = _Bath(b.beta, b.gamma, b.zeta, b.K, None, None, _csr_struct(*b.v_csr, keep))
             continue
         if b.v_diag is None:
@@ -321,6 +326,8 @@ class Context:
         self.dim = d
         # device slabs hold the upper triangle only (see herm_index)
         self.hermitian_packed = (d >= 32 and int(self.info.state_bytes) == self.size * (d * (d + 1) // 2) * 16)
+        # stage kernels in use: "fused", "band", "flip", "csr" or "generic"
+        self.stage_path = STAGE_PATHS[int(self.info.stage_path)]
 
     # lifecycle -----------------------------------------------------------
     def close(self) -> None:

@@ -492,6 +492,39 @@ HostCsr flip_csr(const double* v, const double* w, int d, int logd)
     return o;
 }
 
+// The operator as diag(v) + sum_i w_i sigma_x(i) with real v and w, if it has
+// that form: real entries only, every off-diagonal entry a single-spin flip,
+// each flipped spin present once in every row with one value for all rows.
+bool split_flip(const HostCsr& o, int d, int logd, std::vector<double>& v, std::vector<double>& w)
+{
+    v.assign(d, 0.0);
+    w.assign(logd, 0.0);
+    std::vector<int> count(logd, 0);
+    for (int r = 0; r < d; ++r) {
+        unsigned row_bits = 0;
+        for (int q = o.ptr[r]; q < o.ptr[r + 1]; ++q) {
+            const int c = o.col[q];
+            const double2 a = o.val[q];
+            if (a.y != 0.0) return false;
+            if (c == r) {
+                v[r] += a.x;
+                continue;
+            }
+            const unsigned x = static_cast<unsigned>(r ^ c);
+            if ((x & (x - 1)) != 0) return false;
+            const int bit = __builtin_ctz(x);
+            if (row_bits & x) return false;  // the same flip twice in one row
+            row_bits |= x;
+            if (count[bit] > 0 && w[bit] != a.x) return false;
+            w[bit] = a.x;
+            ++count[bit];
+        }
+    }
+    for (int b = 0; b < logd; ++b)
+        if (count[b] != 0 && count[b] != d) return false;
+    return true;
+}
+
 // Mixed precision: the whole state as complex128 on the host (complex64
 // hierarchy widened, ADO 0 from its double-precision slab); src32/src64 are
 // matching buffers (rho32/rho, ua32/ua, ...).
@@ -600,12 +633,15 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
 
     const int J = static_cast<int>(p->n_baths);
     // general sparse operators: checked and gathered here, run on the CSR path
+    // unless every operator is a diagonal plus single-spin flips (then the
+    // problem is rewritten in that form and takes the faster paths)
     bool use_csr = p->h_csr != nullptr;
     for (int j = 0; j < J; ++j) use_csr = use_csr || p->baths[j].coupling_csr != nullptr;
     std::vector<HostCsr> ops;
+    hx_problem lowered;
+    std::vector<hx_bath> lowered_baths;
+    std::vector<std::vector<double>> lowered_arrays;
     if (use_csr) {
-        if (p->precision != HX_PRECISION_DOUBLE)
-            return fail(HX_ERR_UNSUPPORTED_PRECISION, "sparse operators run in double precision");
         std::string why;
         ops.resize(J + 1);
         if (p->h_csr) {
@@ -624,6 +660,28 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                 if (!b.coupling_diag) return fail(HX_ERR_UNSUPPORTED_BATH, "bath coupling operator is NULL");
                 ops[1 + j] = flip_csr(b.coupling_diag, b.coupling_flip, static_cast<int>(d), logd);
             }
+        }
+        lowered_arrays.resize(2 * (J + 1));
+        bool all_flip = true;
+        for (int k = 0; k <= J && all_flip; ++k)
+            all_flip = split_flip(ops[k], static_cast<int>(d), logd, lowered_arrays[2 * k], lowered_arrays[2 * k + 1]);
+        if (all_flip) {
+            lowered = *p;
+            lowered_baths.assign(p->baths, p->baths + J);
+            lowered.h_csr = nullptr;
+            lowered.h_diag = lowered_arrays[0].data();
+            lowered.h_flip = lowered_arrays[1].data();
+            for (int j = 0; j < J; ++j) {
+                lowered_baths[j].coupling_csr = nullptr;
+                lowered_baths[j].coupling_diag = lowered_arrays[2 * (j + 1)].data();
+                lowered_baths[j].coupling_flip = lowered_arrays[2 * (j + 1) + 1].data();
+            }
+            lowered.baths = lowered_baths.data();
+            p = &lowered;
+            use_csr = false;
+            ops.clear();
+        } else if (p->precision != HX_PRECISION_DOUBLE) {
+            return fail(HX_ERR_UNSUPPORTED_PRECISION, "sparse operators run in double precision");
         }
     }
     std::vector<hx::BathConst> bc(J);
@@ -922,6 +980,11 @@ int hx_ctx_info(const hx_ctx* c, hx_info* info)
     int per_stage = (c->use_flip || c->use_csr || (c->use_fused && c->up_slots > 0)) ? 2 : 1;
     if (c->use_large) per_stage = 1 + (c->up_slots > 0 ? 1 : 0) + (c->mixed ? 1 : 0);
     info->kernels_per_step = static_cast<uint32_t>(c->order) * per_stage;
+    info->stage_path = c->use_csr ? HX_PATH_CSR
+                       : c->use_flip ? HX_PATH_FLIP
+                       : c->use_large ? HX_PATH_BAND
+                       : c->use_fused ? HX_PATH_FUSED
+                       : HX_PATH_GENERIC;
     return HX_OK;
 }
 

@@ -121,7 +121,17 @@ typedef struct hx_info {
     uint64_t steps_done;
     double time;                /* steps_done * dt */
     uint32_t kernels_per_step;  /* kernel launches one step enqueues */
+    uint32_t stage_path;        /* HX_PATH_*: the stage kernels this context runs */
 } hx_info;
+
+/* hx_info.stage_path.  Sparse operators (hx_csr) that are a real diagonal
+ * plus single-spin flips of one weight per spin are rewritten in that form
+ * at creation and take the flip, fused or band path. */
+#define HX_PATH_GENERIC 0u  /* stage_kernel: d <= 64 outside the fused shapes */
+#define HX_PATH_FUSED 1u    /* herm_kernel / fused_kernel (+ upterm_kernel): d = 32, 64 */
+#define HX_PATH_BAND 2u     /* band kernels: 128 <= d <= 1024, diagonal couplings */
+#define HX_PATH_FLIP 3u     /* comm_kernel + combine_kernel: couplings with spin flips */
+#define HX_PATH_CSR 4u      /* csr_comm_kernel + csr_combine_kernel: general sparse operators */
 
 /* Profiling counters (replaces src/library/backend_profiling.cpp:9-137). */
 typedef struct hx_counters {

@@ -20,6 +20,7 @@ def test_legacy_model_rhs_and_steps_match_oracle(dim):
     o = O.Oracle(p)
     with capi.Context(p) as ctx:
         assert ctx.size == 10
+        assert ctx.stage_path == "flip"
         rng = np.random.default_rng(dim)
         x = rng.standard_normal((10, dim, dim)) + 1j * rng.standard_normal((10, dim, dim))
         ctx.set_state(x)
@@ -40,6 +41,7 @@ def test_legacy_compiled_default_energy_trace(golden):
     g = golden("legacy_energy_trace.json")
     p = S.legacy_spin_glass(1024)
     with capi.Context(p) as ctx:
+        assert ctx.stage_path == "flip"
         e0, tr = ctx.observables()
         assert abs(e0 - g["energy"][0]) < 1e-5 and abs(tr - 1.0) < 1e-14
         rho, en = ctx.step_trace(40, rho0=True)

@@ -2,6 +2,8 @@
 compressed rows, the System::from_sparse case the reference validates but
 does not execute) on the CSR stage kernels (hx_csr.cu), against the FP64
 oracle, which takes the same CSR operators.  Bars as in test_gpu_parity.py."""
+import copy
+
 import numpy as np
 import pytest
 
@@ -21,6 +23,7 @@ def test_sparse_rhs_and_trajectory_match_oracle(n, depth, K):
     with capi.Context(p) as ctx:
         assert ctx.size == o.size
         assert not ctx.hermitian_packed
+        assert ctx.stage_path == "csr"
         assert ctx.get_info().kernels_per_step == 8  # two kernels per stage
         rng = np.random.default_rng(n)
         x = rng.standard_normal((ctx.size, p.dim, p.dim)) + 1j * rng.standard_normal((ctx.size, p.dim, p.dim))
@@ -50,8 +53,45 @@ def test_sparse_hamiltonian_with_diagonal_couplings_d32():
     o = O.Oracle(p)
     with capi.Context(p) as ctx:
         assert not ctx.hermitian_packed
+        assert ctx.stage_path == "csr"
         rho, en = ctx.step_trace(10)
     rho_ref, en_ref = o.run(10, trace=True)
     o.close()
     assert np.max(np.abs(rho - rho_ref)) <= TOL
     assert np.max(np.abs(en - en_ref)) <= TOL
+
+
+def _as_csr_only(p):
+    """The same problem with H and every V_j passed in compressed rows only."""
+    q = copy.deepcopy(p)
+    q.h_csr_explicit = p.h_csr()
+    for j, b in enumerate(q.baths):
+        b.v_csr = p.bath_csr(j)
+        b.v_diag = None
+        b.v_flip = None
+    return q
+
+
+@pytest.mark.parametrize("case", ["spin_glass_d32", "spin_glass_d128", "legacy_d64"])
+def test_flip_form_csr_operators_take_the_fast_paths(case):
+    """CSR operators that are a real diagonal plus single-spin flips are
+    rewritten at creation: the same stage path and bit-identical states as
+    the diagonal / flip-weight form of the same problem."""
+    if case == "spin_glass_d32":
+        p, path = S.spin_glass(5, seed=41, depth=2, K=1, h=0.6, dt=0.005), "fused"
+    elif case == "spin_glass_d128":
+        p, path = S.spin_glass(7, seed=42, depth=1, K=1, h=0.6, dt=0.005), "band"
+    else:
+        p, path = S.legacy_spin_glass(64), "flip"
+    q = _as_csr_only(p)
+    with capi.Context(p) as a, capi.Context(q) as b:
+        assert a.stage_path == path and b.stage_path == path
+        assert a.hermitian_packed == b.hermitian_packed
+        ra, ea = a.step_trace(6)
+        rb, eb = b.step_trace(6)
+    assert np.array_equal(ra, rb) and np.array_equal(ea, eb)
+    o = O.Oracle(q)
+    rho_ref, en_ref = o.run(6, trace=True)
+    o.close()
+    assert np.max(np.abs(rb - rho_ref)) <= TOL
+    assert np.max(np.abs(eb - en_ref)) <= TOL
