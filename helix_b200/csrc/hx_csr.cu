@@ -10,11 +10,12 @@
 //   (X A)_rc = sum_k X_rk A_kc = sum_{p in row c} X_{r, col p} conj(A_p)
 // so both sides of a commutator use the rows of A.  As in the flip path
 // (hx_flip.cu) each stage runs in two passes:
-//   csr_comm_kernel:    B_{j,n} = [V_j, u_n] for every bath j and ADO n
+//   csr_comm_kernel:    B_{j,n} = [V_j, u_n] and A_{j,n} = {V_j, u_n} for
+//                       every bath j and ADO n (B for all (j, n), then A)
 //   csr_combine_kernel: out_n = base_n + alpha * ( -i[H,u_n] - g_n u_n
 //                         - i sum_{m up} B_{j(m), n+e_m}
 //                         - i sum_{m down} a_{n,m} B_{j(m), n-e_m}
-//                         - sum_j b_{n,j} {V_j, u_{n-e_j0}}
+//                         - sum_j b_{n,j} A_{j, n-e_j0}
 //                         + sum_j ((-Xi_j - i kappa_j) V_j B_{j,n} + (Xi_j - i kappa_j) B_{j,n} V_j) )
 // the last line being -Xi [V, B] - i kappa {V, B}.  One thread per element;
 // the gathered rows and columns of a slab are read through L1/L2.
@@ -71,16 +72,19 @@ __global__ void __launch_bounds__(256) csr_comm_kernel(CsrArgs a, const double2*
 {
     const int D = 1 << a.logd;
     const long long D2 = static_cast<long long>(D) * D;
-    const long long total = static_cast<long long>(a.J) * a.H * D2;
-    for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
-         idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const int j = static_cast<int>(idx / (a.H * D2));
-        const long long rem = idx - static_cast<long long>(j) * a.H * D2;
-        const long long n = rem / D2;
-        const long long e = rem - n * D2;
+    const long long HD2 = a.H * D2;
+    const long long total = static_cast<long long>(a.J) * HD2;
+    for (long long ne = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; ne < HD2;
+         ne += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long n = ne >> (2 * a.logd);
+        const long long e = ne & (D2 - 1);
         const int r = static_cast<int>(e >> a.logd), c = static_cast<int>(e & (D - 1));
-        const Sides s = sides(a, 1 + j, u + n * D2, r, c);
-        B[idx] = make_double2(s.left.x - s.right.x, s.left.y - s.right.y);
+        for (int j = 0; j < a.J; ++j) {
+            const Sides s = sides(a, 1 + j, u + n * D2, r, c);
+            const long long idx = static_cast<long long>(j) * HD2 + ne;
+            B[idx] = make_double2(s.left.x - s.right.x, s.left.y - s.right.y);
+            B[total + idx] = make_double2(s.left.x + s.right.x, s.left.y + s.right.y);
+        }
     }
 }
 
@@ -94,8 +98,8 @@ __global__ void __launch_bounds__(256)
     const long long HD2 = a.H * D2;
     for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
          idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const long long n = idx / D2;
-        const long long e = idx - n * D2;
+        const long long n = idx >> (2 * a.logd);
+        const long long e = idx & (D2 - 1);
         const int r = static_cast<int>(e >> a.logd), c = static_cast<int>(e & (D - 1));
         const double2* un = u + n * D2;
         const double2 x = un[e];
@@ -127,13 +131,13 @@ __global__ void __launch_bounds__(256)
             }
             re += si;
             im -= sr;
-            // theta2: -b {V_j, u_{n-e_j0}}
+            // theta2: -b {V_j, u_{n-e_j0}} = -b A_{j, n-e_j0}
             const int dn0 = edges[a.M + a.bath_off[j]];
             if (dn0 < a.H) {
                 const double b = a.bcoef[n * a.J + j];
-                const Sides s = sides(a, 1 + j, u + static_cast<long long>(dn0) * D2, r, c);
-                re -= b * (s.left.x + s.right.x);
-                im -= b * (s.left.y + s.right.y);
+                const double2 y = __ldg(Bj + static_cast<long long>(a.J) * HD2 + static_cast<long long>(dn0) * D2 + e);
+                re -= b * y.x;
+                im -= b * y.y;
             }
             // -Xi [V, B_n] - i kappa {V, B_n} = (-Xi - i kappa) V B + (Xi - i kappa) B V
             const double xi = a.xi[j], ka = a.counter[j];
@@ -190,7 +194,7 @@ void launch_csr_stage(const CsrArgs& a, const double2* u, double2* B, const doub
                       int base_kind, cudaStream_t s)
 {
     const long long D2 = 1ll << (2 * a.logd);
-    csr_comm_kernel<<<grid_for(static_cast<long long>(a.J) * a.H * D2), 256, 0, s>>>(a, u, B);
+    csr_comm_kernel<<<grid_for(a.H * D2), 256, 0, s>>>(a, u, B);
     csr_combine_kernel<<<grid_for(a.H * D2), 256, 0, s>>>(a, u, B, rho, out, alpha, base_kind);
 }
 

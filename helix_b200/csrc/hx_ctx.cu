@@ -751,7 +751,8 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     c->slab_store = c->herm ? static_cast<size_t>(hx::herm_elems(logd)) : c->slab;
     const size_t nstate = static_cast<size_t>(H) * c->slab_store;
     if ((rc = dev_alloc(c, &c->vflip, vf.size())) || (rc = upload(c, c->vflip, vf))) return bail(rc);
-    if ((c->use_flip || c->use_csr) && (rc = dev_alloc(c, &c->Bbuf, nstate * J))) return bail(rc);
+    // two-pass paths: [V_j, u_n] and {V_j, u_n} for every bath and ADO
+    if ((c->use_flip || c->use_csr) && (rc = dev_alloc(c, &c->Bbuf, 2 * nstate * J))) return bail(rc);
     if (c->use_csr) {
         std::vector<int32_t> ptr, col;
         std::vector<double2> val;

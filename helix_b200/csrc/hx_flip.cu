@@ -10,12 +10,14 @@
 //
 // so, as in the reference (getdRhoSparse, src/liouville.cu:778-860), each
 // stage runs in two passes:
-//   comm_kernel:     B_{j,n} = [V_j, u_n] for every bath j and ADO n
+//   comm_kernel:     B_{j,n} = [V_j, u_n] and A_{j,n} = {V_j, u_n} for every
+//                    bath j and ADO n (both from the same flip loads)
 //   combine_kernel:  out_n = base_n + alpha * ( -i[H,u_n] - g_n u_n
 //                      - i sum_{m up} B_{j(m), n+e_m}
 //                      - i sum_{m down} a_{n,m} B_{j(m), n-e_m}
-//                      - sum_j b_{n,j} {V_j, u_{n-e_j0}}
+//                      - sum_j b_{n,j} A_{j, n-e_j0}
 //                      - sum_j (Xi_j [V_j, B_{j,n}] + i kappa_j {V_j, B_{j,n}}) )
+// The buffer holds B for all (j, n), then A for all (j, n).
 // One thread per element, flip partners read through L1/L2 (a slab of
 // d = 1024 is 16 MB and stays in L2 while its rows are processed).
 
@@ -34,27 +36,34 @@ __global__ void __launch_bounds__(256)
 {
     const int D = 1 << a.logd;
     const long long D2 = static_cast<long long>(D) * D;
-    const long long total = static_cast<long long>(a.J) * a.H * D2;
-    for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
-         idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const int j = static_cast<int>(idx / (a.H * D2));
-        const long long rem = idx - static_cast<long long>(j) * a.H * D2;
-        const long long n = rem / D2;
-        const long long e = rem - n * D2;
+    const long long HD2 = a.H * D2;
+    const long long total = static_cast<long long>(a.J) * HD2;
+    for (long long ne = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; ne < HD2;
+         ne += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long n = ne >> (2 * a.logd);
+        const long long e = ne & (D2 - 1);
         const int r = static_cast<int>(e >> a.logd), c = static_cast<int>(e & (D - 1));
         const double2* un = u + n * D2;
         const double2 x = un[e];
-        const double del = a.vdiag[j * D + r] - a.vdiag[j * D + c];
-        double re = del * x.x, im = del * x.y;
-        for (int i = 0; i < a.logd; ++i) {
-            const double w = a.vflip[j * a.logd + i];
-            if (w == 0.0) continue;
-            const double2 pr = __ldg(un + (e ^ (static_cast<long long>(1) << (i + a.logd))));
-            const double2 pc = __ldg(un + (e ^ (static_cast<long long>(1) << i)));
-            re += w * (pr.x - pc.x);
-            im += w * (pr.y - pc.y);
+        for (int j = 0; j < a.J; ++j) {
+            const double vr = a.vdiag[j * D + r], vc = a.vdiag[j * D + c];
+            const double del = vr - vc, sum = vr + vc;
+            double re = del * x.x, im = del * x.y;
+            double ar = sum * x.x, ai = sum * x.y;
+            for (int i = 0; i < a.logd; ++i) {
+                const double w = a.vflip[j * a.logd + i];
+                if (w == 0.0) continue;
+                const double2 pr = __ldg(un + (e ^ (static_cast<long long>(1) << (i + a.logd))));
+                const double2 pc = __ldg(un + (e ^ (static_cast<long long>(1) << i)));
+                re += w * (pr.x - pc.x);
+                im += w * (pr.y - pc.y);
+                ar += w * (pr.x + pc.x);
+                ai += w * (pr.y + pc.y);
+            }
+            const long long idx = static_cast<long long>(j) * HD2 + ne;
+            B[idx] = make_double2(re, im);
+            B[total + idx] = make_double2(ar, ai);
         }
-        B[idx] = make_double2(re, im);
     }
 }
 
@@ -68,8 +77,8 @@ __global__ void __launch_bounds__(256)
     const long long HD2 = a.H * D2;
     for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
          idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const long long n = idx / D2;
-        const long long e = idx - n * D2;
+        const long long n = idx >> (2 * a.logd);
+        const long long e = idx & (D2 - 1);
         const int r = static_cast<int>(e >> a.logd), c = static_cast<int>(e & (D - 1));
         const double2* un = u + n * D2;
         const double2 x = un[e];
@@ -114,23 +123,13 @@ __global__ void __launch_bounds__(256)
             }
             re += si;
             im -= sr;
-            // theta2: -b {V_j, u_{n-e_j0}}
+            // theta2: -b {V_j, u_{n-e_j0}} = -b A_{j, n-e_j0}
             const int dn0 = edges[a.M + a.bath_off[j]];
             if (dn0 < a.H) {
                 const double b = a.bcoef[n * a.J + j];
-                const double2* ud = u + static_cast<long long>(dn0) * D2;
-                const double2 y = __ldg(ud + e);
-                double ar = (vr + vc) * y.x, ai = (vr + vc) * y.y;
-                for (int i = 0; i < a.logd; ++i) {
-                    const double w = a.vflip[j * a.logd + i];
-                    if (w == 0.0) continue;
-                    const double2 pr = __ldg(ud + (e ^ (static_cast<long long>(1) << (i + a.logd))));
-                    const double2 pc = __ldg(ud + (e ^ (static_cast<long long>(1) << i)));
-                    ar += w * (pr.x + pc.x);
-                    ai += w * (pr.y + pc.y);
-                }
-                re -= b * ar;
-                im -= b * ai;
+                const double2 y = __ldg(Bj + static_cast<long long>(a.J) * HD2 + static_cast<long long>(dn0) * D2 + e);
+                re -= b * y.x;
+                im -= b * y.y;
             }
             // Xi and counter: -Xi [V, B_n] - i kappa {V, B_n}
             const double xi = a.xi[j], ka = a.counter[j];
@@ -163,13 +162,12 @@ void launch_flip_stage(const FlipArgs& a, const double2* u, double2* B, const do
                        double alpha, int base_kind, cudaStream_t s)
 {
     const long long D2 = 1ll << (2 * a.logd);
-    const long long nb = static_cast<long long>(a.J) * a.H * D2;
     const long long nc = a.H * D2;
     auto grid_for = [](long long n) {
         long long g = (n + 255) / 256;
         return static_cast<unsigned>(g < 148ll * 64 ? g : 148ll * 64);
     };
-    comm_kernel<<<grid_for(nb), 256, 0, s>>>(a, u, B);
+    comm_kernel<<<grid_for(nc), 256, 0, s>>>(a, u, B);
     combine_kernel<<<grid_for(nc), 256, 0, s>>>(a, u, B, rho, out, alpha, base_kind);
 }
 

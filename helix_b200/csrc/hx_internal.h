@@ -252,7 +252,7 @@ struct FlipArgs {
     long long H;
     int M, J, logd;
 };
-// B (J * H * d*d complex) receives [V_j, u_n]; then out = base + alpha L(u).
+// B (2 J H d*d complex) receives [V_j, u_n], then {V_j, u_n}; then out = base + alpha L(u).
 void launch_flip_stage(const FlipArgs& a, const double2* u, double2* B, const double2* rho, double2* out,
                        double alpha, int base_kind, cudaStream_t s);
 
@@ -341,7 +341,7 @@ struct hx_ctx {
     float2* diag32 = nullptr;
     float* vdiag32 = nullptr;
     float* hflip32 = nullptr;
-    double2* Bbuf = nullptr;      // [J][H][d*d] commutators [V_j, u_n] (flip path)
+    double2* Bbuf = nullptr;      // [2][J][H][d*d] [V_j, u_n] then {V_j, u_n} (flip and CSR paths)
     double* xi = nullptr;
     double* counter = nullptr;
     int32_t* bath_off = nullptr;
