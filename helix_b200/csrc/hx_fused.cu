@@ -339,13 +339,14 @@ __device__ __forceinline__ void herm_ado(const FusedArgs& a, long long n, const 
 
     const int tid = threadIdx.x;
     const uint64_t pkeep = pol_last(), pn = pol_normal();
+    // thread 0 alone owns the two mbarriers (init, copies, waits); the others
+    // learn of a completed copy from the block barrier that follows its wait
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(&bar[0])) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(&bar[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        bulk_g2s(pk, u + n * P, P * sizeof(double2), &bar[0], a.ado_keep[n] ? pkeep : pn);
     }
-    __syncthreads();
-    if (tid == 0) bulk_g2s(pk, u + n * P, P * sizeof(double2), &bar[0], a.ado_keep[n] ? pkeep : pn);
     const int Q = a.ent_count[n];
     if (PAULI) {
         if (tid < a.J) sBit[tid] = a.vbit[tid];
@@ -362,8 +363,8 @@ __device__ __forceinline__ void herm_ado(const FusedArgs& a, long long n, const 
     }
     const double g = a.gsum[n];
     const int slot = a.slot ? a.slot[n] : -1;
-    __syncthreads();
-    if (__syncthreads_or(!bar_wait(&bar[0], 0))) {
+    // one barrier publishes the tables above and the arrival of the slab
+    if (__syncthreads_or(tid == 0 && !bar_wait(&bar[0], 0))) {
         if (tid == 0) atomicExch(a.error_flag, 1);
         return;
     }
@@ -474,7 +475,7 @@ __device__ __forceinline__ void herm_ado(const FusedArgs& a, long long n, const 
     }
 
     // ---- Horner epilogue
-    if (base_kind == kBaseRho && __syncthreads_or(!bar_wait(&bar[1], 0))) {
+    if (base_kind == kBaseRho && __syncthreads_or(tid == 0 && !bar_wait(&bar[1], 0))) {
         if (tid == 0) atomicExch(a.error_flag, 1);
         return;
     }
