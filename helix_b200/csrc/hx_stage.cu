@@ -111,9 +111,10 @@ __global__ void __launch_bounds__(256) stage_kernel(StageTables t, const double2
 
     const long long n = t.order ? static_cast<long long>(t.order[blockIdx.x]) : static_cast<long long>(blockIdx.x);
     const long long H = t.H;
-    if (threadIdx.x == 0) mbar_init(bar, 1);
-    __syncthreads();
+    // thread 0 alone owns the mbarrier (init, copy, wait); the others learn of
+    // the slab's arrival from the block barrier that follows its wait
     if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
         mbar_expect_tx(bar, D2 * sizeof(double2));
         bulk_load(su, u + n * D2, D2 * sizeof(double2), bar);
     }
@@ -132,9 +133,9 @@ __global__ void __launch_bounds__(256) stage_kernel(StageTables t, const double2
         sDn[i] = t.edges[n * 2 * M + M + i];
     }
     const double g = t.gsum[n];
-    __syncthreads();
-    if (!mbar_wait_bounded(bar, 0, kWaitLimit)) {
-        atomicExch(t.error_flag, 1);
+    // one barrier publishes the tables above and the arrival of the slab
+    if (__syncthreads_or(threadIdx.x == 0 && !mbar_wait_bounded(bar, 0, kWaitLimit))) {
+        if (threadIdx.x == 0) atomicExch(t.error_flag, 1);
         return;
     }
 
