@@ -1,7 +1,7 @@
 """Build recipes for the test-only oracle libraries.
 
 * ``oracle/_build/liboracle.so`` — the FP64 CPU restatement in
-  ``oracle/heom_oracle.cpp`` (g++ -O3 -march=native -fopenmp).
+  ``oracle/heom_oracle.cpp`` (g++ -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp).
 * ``oracle/_ref/libhelix_ref_host.so`` — the reference's own host-side setup
   code (hierarchy tables, Pade decomposition, legacy operator helpers) compiled
   from the reference tree with ``oracle/ref_host_shim.cu``.  Built only where

@@ -19,7 +19,7 @@
 // functions compiled from source (oracle/ref_host_shim.cu), and the
 // legacy-model energy trace against examples/outputEnergy.txt.
 //
-// Build: g++ -O3 -march=native -fopenmp -shared -fPIC (see oracle/build.py).
+// Build: g++ -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp -shared -fPIC (oracle/build.py).
 
 #include <algorithm>
 #include <cmath>
