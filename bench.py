@@ -529,12 +529,13 @@ def run_batch(args, cfg: dict) -> None:
     peak, peak_kind = load_peaks()
     b.close()
 
-    # end to end through the public API: create from host problems, step with
+    # end to end through the public API: create from host problems (tuned, as
+    # for the device-timed run), step with
     # the per-step disorder-average trace copied to the host, all-reduce
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    b = capi.Batch(mine)
+    b = capi.Batch(mine, tune=True)
     sz = b.step(args.steps)
     b.close()
     tot = torch.tensor(np.concatenate([sz, [len(mine)]]), device="cuda")
@@ -612,7 +613,8 @@ def run_batch(args, cfg: dict) -> None:
                          "launch_ms": stage_ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": 8,
-                    "path": "hx_batch_create (host problems) + hx_batch_step (<sigma_z> sum per step to host) + all-reduce"},
+                    "path": "hx_batch_create (host problems, with the tile autotuner) + hx_batch_step "
+                            "(<sigma_z> sum per step to host) + all-reduce"},
             "gpu_launches": launches,
             "clocks": clk,
             "disorder_average_sz_final": float(mean_sz[-1]),
