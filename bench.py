@@ -355,10 +355,10 @@ def run_ours(args, cfg: dict) -> None:
         ctx.step(1)
     ctx.sync()
     c0 = ctx.counters()
-    barrier()
-    torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
+    barrier()
+    torch.cuda.synchronize()
     if small:
         ms = flusher.time_steps(lambda: ctx.step(1), args.steps)
     else:
@@ -507,10 +507,10 @@ def run_batch(args, cfg: dict) -> None:
     b.step(args.warmup, trace=False)
     b.sync()
     l0 = int(b.info().kernel_launches)
-    barrier()
-    torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
+    barrier()
+    torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
