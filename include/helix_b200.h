@@ -105,9 +105,11 @@ typedef struct hx_problem {
 
 /* Every ADO of this hierarchy stays Hermitian (H and the V_j are Hermitian
  * and every term of the right-hand side maps Hermitian matrices to Hermitian
- * matrices), so for d = 32 ... 1024 the device state (complex64 in mixed
- * precision) keeps the upper triangle of each slab only (d(d+1)/2 elements instead of
- * d^2), which halves the memory traffic of a step.  The C ABI still reads and writes full d x d
+ * matrices), so for d = 32 ... 1024 with diagonal coupling operators (the
+ * fused and band paths) the device state (complex64 in mixed precision) keeps
+ * the upper triangle of each slab only (d(d+1)/2 elements instead of d^2),
+ * which halves the memory traffic of a step; the flip and CSR paths keep
+ * full slabs.  The C ABI still reads and writes full d x d
  * slabs; hx_ctx_write_state then rejects non-Hermitian ADOs.  This flag keeps
  * full slabs on the device, for general (non-Hermitian) states. */
 #define HX_FLAG_FULL_STATE 1u
