@@ -60,6 +60,32 @@ def make_problem(cfg: dict, rank: int = 0):
                         dt=cfg["dt"])
 
 
+L2_BYTES_NOMINAL = 126 * 2**20  # B200 L2 (the timing code reads the device's own figure)
+
+
+def workload_config(cfg: dict, p, world: int) -> dict:
+    """The `config` object of the JSON line, identical in both arms: it
+    describes the workload (one hierarchy per rank), not the implementation."""
+    H = p.hierarchy_size()
+    full_bytes = H * p.dim * p.dim * 16
+    small = full_bytes < L2_BYTES_NOMINAL
+    return {"workload": cfg["workload"], "ados": H, "dim": p.dim, "modes": p.modes, "depth_L": p.max_depth - 1,
+            "dt": p.dt, "integrator": "RK4 (4-term Taylor, Horner form)",
+            "parallelism": f"{world} independent replicas" if world > 1 else "single",
+            "l2": ("L2 flushed before every timed step (the state fits in L2; steps timed one by one with "
+                   "CUDA events, the flush outside the events)") if small
+            else f"inputs larger than L2 (hierarchy {H} x {p.dim} x {p.dim} complex128)"}
+
+
+def batch_config(cfg: dict, problems, world: int) -> dict:
+    """The `config` object of the batched workload, identical in both arms."""
+    return {"workload": cfg["workload"], "instances": len(problems),
+            "ados": sum(q.hierarchy_size() for q in problems), "dt": cfg["dt"],
+            "integrator": "RK4 (4-term Taylor, Horner form)",
+            "parallelism": f"instances sharded over {world} rank(s)" if world > 1 else "single",
+            "l2": "inputs larger than L2 (all instances' states)"}
+
+
 def load_peaks() -> tuple[float, str]:
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -215,6 +241,47 @@ def stage_kernels_label(ctx, p, packed: bool, per_stage: int) -> str:
     return "stage_kernel per stage (generic path)"
 
 
+def reference_cuda(cfg: dict, p, steps: int) -> dict:
+    """Time the reference's own CUDA propagator (oracle/_ref/ref_cuda_propagator:
+    its initialize() + develop() with cuSPARSE/cuBLAS, built from its sources for
+    sm_100a in FP64) at this workload's work shape: d, modes (one collective
+    bath with modes - 1 Pade poles) and depth bound as the workload, on the
+    reference's own model (collective V with sigma_x flips, diagonal H).  Same
+    ADOs, same neighbour terms per ADO, same integrator; the physics differs
+    (the reference fixes its model at compile time).  CUDA events on the
+    legacy default stream around K develop() calls after a warm-up step."""
+    from oracle import build as ob
+
+    res = {"unit": UNIT, "shape": {"dim": p.dim, "modes": p.modes, "max_depth": p.max_depth, "dt": p.dt}}
+    H = p.hierarchy_size()
+    k = 3 if H > 1000 else max(3, min(steps, 50))
+    out = {}
+    for name, binary in (("fp64", ob.REF_CUDA_BIN), ("fp32", ob.REF_CUDA_BIN_FP32)):
+        if name == "fp32" and not cfg.get("legacy"):
+            continue
+        if not os.path.exists(binary):
+            out[name] = {"unavailable": f"{os.path.relpath(binary, ROOT)} not built (needs the reference tree)"}
+            continue
+        env = dict(os.environ, HX_REF_DIM=str(p.dim), HX_REF_KMAX=str(p.modes - 1), HX_REF_JMAX=str(p.max_depth),
+                   HX_REF_DT=repr(p.dt), CUBLAS_WORKSPACE_CONFIG=":16:8")
+        try:
+            r = subprocess.run([binary, "--time", str(k), "--warmup", "1"], env=env, capture_output=True,
+                               text=True, timeout=900)
+            line = json.loads(r.stdout.strip().splitlines()[-1])
+        except (subprocess.SubprocessError, ValueError, IndexError) as e:
+            out[name] = {"unavailable": f"run failed: {type(e).__name__}"}
+            continue
+        if r.returncode != 0 or line.get("cuda_error"):
+            out[name] = {"unavailable": f"exit {r.returncode}: {line.get('cuda_error', '')}"}
+            continue
+        out[name] = {"value": line["ado_steps_per_s"], "ms_per_step": line["ms_per_step"],
+                     "wall_ms_per_step": line["wall_ms_per_step"], "steps": line["timed_steps"],
+                     "ados": line["hierarchy_size"], "init_ms": line["init_ms"],
+                     "device_bytes_in_use": line["device_bytes_in_use"]}
+    res.update(out)
+    return res
+
+
 def cpu_model() -> str:
     try:
         with open("/proc/cpuinfo") as f:
@@ -251,6 +318,7 @@ def cpu_baseline(cfg: dict, steps: int) -> dict:
 
 
 REFERENCE_BUDGET_S = 60.0  # timed CPU work of the reference arm
+MIN_WINDOWS, MAX_WINDOWS, WINDOW_TARGET_MS = 5, 200, 1000.0  # repeats of the timed --steps window
 
 
 def timed_steps(step_all, steps: int, budget_s: float = REFERENCE_BUDGET_S) -> tuple[int, float]:
@@ -291,8 +359,7 @@ def run_reference(args, cfg: dict) -> None:
             "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": n, "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec / n,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "ados": size, "instances": len(sample), "dt": cfg["dt"],
-                       "parallelism": "host threads"},
+            "config": batch_config(cfg, S.disorder_batch(cfg["count"], cfg["seed"], dt=cfg["dt"]), args.gpus),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.threads(), "kind": "port",
                              "sample": f"{len(sample)} instances (<= 1000 ADOs each), {n} steps; the "
                                        "reference has no CPU path, so its FP64 restatement stands in"},
@@ -311,8 +378,7 @@ def run_reference(args, cfg: dict) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": n, "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec / n,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "ados": o.size, "dim": p.dim, "modes": p.modes,
-                   "dt": p.dt, "parallelism": "host threads"},
+        "config": workload_config(cfg, p, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{n} full steps of the {o.size}-ADO hierarchy; the reference has no "
                                    "CPU path, so its FP64 restatement (oracle/heom_oracle.cpp) stands in"},
@@ -350,7 +416,7 @@ def run_ours(args, cfg: dict) -> None:
     # ---- device-resident throughput (value) --------------------------------
     # a state smaller than L2 is timed step by step with L2 flushed in between
     flusher = L2Flush(stream, local)
-    small = state_bytes < flusher.l2_bytes
+    small = H * p.dim * p.dim * 16 < L2_BYTES_NOMINAL  # as workload_config states it
     for _ in range(args.warmup):
         ctx.step(1)
     ctx.sync()
@@ -359,9 +425,11 @@ def run_ours(args, cfg: dict) -> None:
     clocks.start()
     barrier()
     torch.cuda.synchronize()
-    if small:
-        ms = flusher.time_steps(lambda: ctx.step(1), args.steps)
-    else:
+
+    def window() -> float:
+        """Device time (ms) of one window of --steps steps."""
+        if small:
+            return flusher.time_steps(lambda: ctx.step(1), args.steps)
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
@@ -369,11 +437,25 @@ def run_ours(args, cfg: dict) -> None:
         ev1.record(stream)
         ctx.sync()
         torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1)
+        return ev0.elapsed_time(ev1)
+
+    # the --steps window is repeated (every rank the same number of times,
+    # fixed by rank 0's first window) until about 1 s of device time has
+    # passed, so the clock sampler sees the GPU under load; ms = the median
+    # window
+    windows = [window()]
+    reps = max(MIN_WINDOWS, min(MAX_WINDOWS, int(np.ceil(WINDOW_TARGET_MS / max(windows[0], 1e-3)))))
+    if world > 1:
+        t = torch.tensor([reps], device="cuda")
+        dist.broadcast(t, 0)
+        reps = int(t.item())
+    for _ in range(reps - 1):
+        windows.append(window())
+    ms = float(np.median(windows))
     clk = clocks.stop()
     del flusher
     c1 = ctx.counters()
-    launches = int(c1.kernel_launches - c0.kernel_launches)
+    launches = int(c1.kernel_launches - c0.kernel_launches) // len(windows)
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -428,6 +510,12 @@ def run_ours(args, cfg: dict) -> None:
         cpu = cpu_baseline(cfg, args.cpu_steps)
 
     ctx.close()
+    ref_cuda = None
+    if rank == 0 and world == 1 and not args.no_ref_cuda:
+        ref_cuda = reference_cuda(cfg, p, args.steps)
+        if "value" in ref_cuda.get("fp64", {}):
+            ref_cuda["value_over_fp64_reference"] = value / ref_cuda["fp64"]["value"]
+            ref_cuda["e2e_over_fp64_reference"] = e2e_value / ref_cuda["fp64"]["value"]
     # the reference publishes one number: its compiled default (the legacy
     # workload, FP32, RTX 4070 SUPER): 85.718 ms per step of 10 ADOs
     published = LEGACY_PUBLISHED_ADO_STEPS if cfg.get("legacy") else None
@@ -436,13 +524,9 @@ def run_ours(args, cfg: dict) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": value / published if published else None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "ados": H, "dim": p.dim, "modes": p.modes,
-                       "depth_L": p.max_depth - 1,
-                       "dt": p.dt, "integrator": "RK4 (4-term Taylor, Horner form)",
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": (f"L2 flushed before every timed step (state {state_bytes / 1e6:.1f} MB fits in L2; "
-                              "steps timed one by one with CUDA events, flush outside the events)") if small
-                       else f"inputs larger than L2 (state {state_bytes / 1e9:.3f} GB)"},
+            "config": workload_config(cfg, p, world),
+            "timing": {"windows": len(windows), "window_ms_min": min(windows), "window_ms_max": max(windows),
+                       "statistic": "median device time of the --steps window"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
@@ -461,6 +545,8 @@ def run_ours(args, cfg: dict) -> None:
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if ref_cuda is not None:
+            line["reference_cuda"] = ref_cuda
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -600,11 +686,9 @@ def run_batch(args, cfg: dict) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "instances": len(problems), "ados": total_ados,
-                       "ados_this_rank": ados, "dt": cfg["dt"], "integrator": "RK4 (4-term Taylor, Horner form)",
-                       "parallelism": f"instances sharded over {world} rank(s)" if world > 1 else "single",
-                       "tile_elems": int(st.tile_elems), "threads": int(st.threads), "grid": int(st.grid),
-                       "l2": f"inputs larger than L2 (state {state_bytes / 1e9:.3f} GB per rank)"},
+            "config": batch_config(cfg, problems, world),
+            "batch_layout": {"ados_this_rank": ados, "state_bytes_this_rank": state_bytes,
+                             "tile_elems": int(st.tile_elems), "threads": int(st.threads), "grid": int(st.grid)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
@@ -885,6 +969,8 @@ def main() -> None:
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA propagator at the workload's shape")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":

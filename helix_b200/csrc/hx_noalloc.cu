@@ -17,7 +17,15 @@
 //    HX_ERR_UNSUPPORTED_HIERARCHY and a message that states the size needed;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current and caches it; make
-//    that first call before any stream capture;
+//    that first call before any stream capture.  The cached address belongs
+//    to the device's primary context: after cudaDeviceReset on that device
+//    it is stale, so do not call this entry point again in that process;
+//  * `rho_device` and `drho_device` must be 16-byte aligned (the state is
+//    read by bulk copies) and must not overlap: every block reads other ADOs'
+//    slabs of `rho_device` while others write `drho_device`, so an in-place
+//    call would race; both are checked and rejected with
+//    HX_ERR_INVALID_RUNTIME_OPTION;
+//  * `stream` must belong to the current device (checked);
 //  * all calls share the one array and it keeps the previous call's
 //    contents: every table is rewritten and the error word is cleared at the
 //    start of each call, and two calls that overlap on the GPU (different
@@ -91,6 +99,8 @@ extern "C" int hx_rhs_noalloc(const hx_problem* p, const double* rho_device, dou
     if (p->n_baths == 0 || !p->baths || p->n_baths > static_cast<uint32_t>(hx::kMaxBaths))
         return fail(HX_ERR_UNSUPPORTED_BATH, "1..64 baths are required");
     if (p->max_depth < 1) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "max_depth must be >= 1");
+    if ((reinterpret_cast<uintptr_t>(rho_device) | reinterpret_cast<uintptr_t>(drho_device)) % 16 != 0)
+        return fail(HX_ERR_INVALID_RUNTIME_OPTION, "rho_device and drho_device must be 16-byte aligned");
 
     const int J = static_cast<int>(p->n_baths);
     if (p->h_csr) return fail(HX_ERR_UNSUPPORTED_EXECUTION, "hx_rhs_noalloc takes diagonal plus flip Hamiltonians only");
@@ -118,6 +128,12 @@ extern "C" int hx_rhs_noalloc(const hx_problem* p, const double* rho_device, dou
     int rc = hx_hierarchy_size(static_cast<uint32_t>(M), p->max_depth, &Hu);
     if (rc != HX_OK) return rc;
     const long long H = static_cast<long long>(Hu);
+    {
+        const uintptr_t bytes = static_cast<uintptr_t>(Hu) * d * d * 2 * sizeof(double);
+        const uintptr_t a = reinterpret_cast<uintptr_t>(rho_device), b = reinterpret_cast<uintptr_t>(drho_device);
+        if (a < b + bytes && b < a + bytes)
+            return fail(HX_ERR_INVALID_RUNTIME_OPTION, "rho_device and drho_device must not overlap");
+    }
     const int D = static_cast<int>(p->max_depth);
     const int nmax = M + D + 1;
     const int kcols = M + 1;
@@ -169,6 +185,13 @@ extern "C" int hx_rhs_noalloc(const hx_problem* p, const double* rho_device, dou
                     "hx_rhs_noalloc needs " + std::to_string(sizing.used) + " bytes of scratch for this hierarchy; "
                     "its fixed scratch array holds " + std::to_string(kNoallocScratchBytes) + " bytes");
 
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    {
+        int cur = 0, sdev = 0;
+        HX_CUDA_TRY(cudaGetDevice(&cur));
+        HX_CUDA_TRY(cudaStreamGetDevice(s, &sdev));
+        if (sdev != cur) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "stream belongs to another device than the current one");
+    }
     void* base = nullptr;
     if ((rc = scratch_address(&base)) != HX_OK) return rc;
     Carve cv{static_cast<unsigned char*>(base)};
@@ -192,7 +215,6 @@ extern "C" int hx_rhs_noalloc(const hx_problem* p, const double* rho_device, dou
     auto* d_mk = cv.take<int32_t>(M + J + 1);
     auto* d_flag = cv.take<int>(1);
 
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     auto up = [&](void* dst, const void* src, size_t bytes) {
         return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
     };

@@ -392,15 +392,18 @@ int hx_ctx_set_closure(hx_ctx* ctx, hx_closure* closure);
  * framework that owns every byte of device memory through its own pool, or a
  * process at its device-memory budget): they pass the state `rho_device` and
  * the result `drho_device` (each hierarchy_size * dim * dim complex doubles,
- * device memory they already own) and the stream to run on (NULL = the
- * legacy default stream).  The working tables live in one fixed 8 MiB device
- * array compiled into the library, reserved on every GPU that loads it until
- * the process exits; a problem whose tables need more is rejected with
- * HX_ERR_UNSUPPORTED_HIERARCHY and a message giving the size needed.  The
- * first call on a device looks up that array's device address and caches it:
- * make that first call before any stream capture.  All calls share the array
+ * full row-major slabs, device memory they already own, 16-byte aligned, not
+ * overlapping) and the stream to run on (NULL = the legacy default stream;
+ * it must belong to the current device).  The working tables live in one
+ * fixed 8 MiB device array compiled into the library, reserved on every GPU
+ * that loads it until the process exits; a problem whose tables need more is
+ * rejected with HX_ERR_UNSUPPORTED_HIERARCHY and a message giving the size
+ * needed.  The first call on a device looks up that array's device address
+ * and caches it: make that first call before any stream capture, and make no
+ * call on a device after cudaDeviceReset of it.  All calls share the array
  * (each call rewrites the tables and clears the error word), so calls that
- * overlap on the GPU race.  Returns when the result is complete. */
+ * overlap on the GPU race.  The call synchronizes `stream` and returns when
+ * the result is complete. */
 int hx_rhs_noalloc(const hx_problem* problem, const double* rho_device, double* drho_device, void* stream);
 
 #ifdef __cplusplus

@@ -49,6 +49,7 @@ def _native_libraries():
     hb.build()
     ob.build_oracle()
     ob.build_ref_host()
+    ob.build_ref_cuda()
     yield
 
 

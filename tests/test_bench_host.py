@@ -46,6 +46,9 @@ def test_reference_arm_line_for_the_small_config():
     assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["config"]["workload"] == bench.CONFIGS["c1"]["workload"]
+    # our arm builds its config from the same function: the two arms' config objects are identical
+    cfg = bench.CONFIGS["c1"]
+    assert line["config"] == json.loads(json.dumps(bench.workload_config(cfg, bench.make_problem(cfg), 1)))
 
 
 def test_clock_sampler_reports_its_fields():

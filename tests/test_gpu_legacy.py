@@ -35,22 +35,39 @@ def test_legacy_model_rhs_and_steps_match_oracle(dim):
     o.close()
 
 
-def test_legacy_compiled_default_energy_trace(golden):
-    """d = 1024, 10 ADOs, dt = 0.1: the first 40 rows of the reference's golden
-    trace (FP32 reference, tolerance 1e-5) and 2 steps against the FP64 oracle."""
+def test_legacy_compiled_default_energy_trace(golden, tmp_path):
+    """d = 1024, 10 ADOs, dt = 0.1: all 1980 steps against all 1981 rows of the
+    reference's golden trace (FP32 reference, tolerance 1e-5), the written
+    outputEnergy.txt against the golden lines, and 2 steps against the FP64 oracle."""
     g = golden("legacy_energy_trace.json")
+    want = np.array(g["energy"])
+    assert want.shape == (1981,)
+    steps = want.size - 1
     p = S.legacy_spin_glass(1024)
     with capi.Context(p) as ctx:
         assert ctx.stage_path == "flip"
         e0, tr = ctx.observables()
-        assert abs(e0 - g["energy"][0]) < 1e-5 and abs(tr - 1.0) < 1e-14
-        rho, en = ctx.step_trace(40, rho0=True)
-    assert np.max(np.abs(en - np.array(g["energy"][1:41]))) < 1e-5
+        assert abs(e0 - want[0]) < 1e-5 and abs(tr - 1.0) < 1e-14
+        rho, en = ctx.step_trace(2, rho0=True)
+        _, en_rest = ctx.step_trace(steps - 2, rho0=False)
+    energies = np.concatenate([[e0], en, en_rest])
+    assert np.max(np.abs(energies - want)) < 1e-5
+    # the file: same line count, the time column byte for byte, energies within 1e-5
+    path = tmp_path / "outputEnergy.txt"
+    capi.write_energy_trace(str(path), np.arange(steps + 1) * p.dt, energies)
+    lines = path.read_text().splitlines()
+    assert len(lines) == want.size
+    for mine, ref_t, ref_e in zip(lines, g["time"], want):
+        t_txt, e_txt = mine.split(" ")
+        assert float(t_txt) == pytest.approx(ref_t, abs=1e-12)
+        assert abs(float(e_txt) - ref_e) < 1e-5
+    for mine, ref_line in zip(lines, g["lines"]):
+        assert mine.split(" ")[0] == ref_line.split(" ")[0]
     o = O.Oracle(p)
     rho_ref, en_ref = o.run(2, trace=True)
     o.close()
-    assert np.max(np.abs(rho[:2] - rho_ref)) <= TOL
-    assert np.max(np.abs(en[:2] - en_ref)) <= TOL
+    assert np.max(np.abs(rho - rho_ref)) <= TOL
+    assert np.max(np.abs(en - en_ref)) <= TOL
 
 
 def test_flip_coupling_on_spin_glass_matches_oracle():

@@ -162,33 +162,42 @@ def test_d64_small_hierarchy_steps():
     o.close()
 
 
-def test_c2_full_size_one_step_and_invariants():
-    """The d=64, 18-mode, L=4 (7315 ADO) FP64 workload: one step against the
-    oracle, then size-independent invariants over further steps."""
+def test_c2_full_size_trajectory_and_invariants():
+    """The d=64, 18-mode, L=4 (7315 ADO) FP64 workload: one step from a random
+    Hermitian state populating every tier, then 20 steps from the reference
+    initial state (rho_0 and <H> after every step, every ADO at the end)
+    against the oracle, then size-independent invariants over 30 more steps."""
     p = S.spin_glass(6, seed=2025, depth=4, K=2, h=1.0, dt=0.005)
+    o = O.Oracle(p)
     with capi.Context(p) as ctx:
         assert ctx.size == 7315
         assert ctx.hermitian_packed
-        # populate every tier: start from a random Hermitian state
         x = _random_state(ctx.size, p.dim, 1, hermitian=True) * 1e-3
         x[0] = S.initial_rho0(p.dim)
         ctx.set_state(x)
         ctx.step(1)
         ctx.sync()
         got = ctx.state()
-        o = O.Oracle(p)
         o.set_state(x)
         o.run(1)
-        want = o.state()
-        o.close()
-        assert np.max(np.abs(got - want)) <= TOL
-        # invariants from the reference initial state
-        ctx.set_state(np.concatenate([S.initial_rho0(p.dim)[None], np.zeros((ctx.size - 1, 64, 64))]))
-        rho, en = ctx.step_trace(50)
+        assert np.max(np.abs(got - o.state())) <= TOL
+        # 20 steps from the reference initial state
+        x0 = np.concatenate([S.initial_rho0(p.dim)[None], np.zeros((ctx.size - 1, 64, 64))])
+        ctx.set_state(x0)
+        o.set_state(x0)
+        rho, en = ctx.step_trace(20)
+        st = ctx.state()
+        rho_ref, en_ref = o.run(20, trace=True)
+        assert np.max(np.abs(rho - rho_ref)) <= TOL
+        assert np.max(np.abs(en - en_ref)) <= TOL
+        assert np.max(np.abs(st - o.state())) <= TOL
+        # invariants over 30 more steps
+        rho, en = ctx.step_trace(30)
         tr = np.trace(rho, axis1=1, axis2=2)
         assert np.max(np.abs(tr - 1.0)) < 1e-12
         assert np.max(np.abs(rho - np.conj(np.transpose(rho, (0, 2, 1))))) < 1e-12
         ctx.check_finite()
+    o.close()
 
 
 def test_trace_mode_matches_stepwise_observables():

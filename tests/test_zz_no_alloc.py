@@ -7,14 +7,17 @@ fixed scratch array compiled into the library.  This test calls it through
 the C ABI twice in a row, on two different problems (so the second call runs
 on tables the first call left in the shared array), and checks each result
 against the allocating entry point hx_ctx_rhs within the RHS tolerance used
-by the other parity tests.  Collected last on purpose (file name), and
-independent of earlier tests.
+by the other parity tests; then at d = 32 and d = 64 (the larger stage
+kernels) against the FP64 oracle, and the argument checks that reject
+misaligned or overlapping buffers before any device work.  Collected last on
+purpose (file name), and independent of earlier tests.
 """
 import numpy as np
 import pytest
 
 from helix_b200 import capi
 from helix_b200 import systems as S
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -53,3 +56,40 @@ def test_rhs_noalloc_rejects_hierarchies_beyond_its_scratch():
         capi.rhs_noalloc(big, 1, 1, 0)  # rejected before any device access
     assert err.value.status == "UnsupportedHierarchy"
     assert "bytes of scratch" in str(err.value)
+
+
+@pytest.mark.parametrize("n,seed,depth,K,h", [(5, 11, 2, 2, 0.7), (6, 12, 2, 1, 0.9)])
+def test_rhs_noalloc_matches_oracle_at_d32_d64(n, seed, depth, K, h):
+    """d = 32 (136 ADOs) and d = 64 (91 ADOs): full slabs of a random complex
+    state against the oracle's right-hand side, two calls in a row."""
+    import torch
+
+    p = S.spin_glass(n, seed=seed, depth=depth, K=K, h=h)
+    o = O.Oracle(p)
+    rng = np.random.default_rng(seed)
+    for _ in range(2):
+        x = (rng.standard_normal((o.size, p.dim, p.dim)) + 1j * rng.standard_normal((o.size, p.dim, p.dim)))
+        want = o.rhs(x)
+        xd = torch.from_numpy(x.reshape(-1)).to("cuda")
+        out = torch.full_like(xd, complex("nan"))
+        torch.cuda.synchronize()
+        capi.rhs_noalloc(p, xd.data_ptr(), out.data_ptr(), 0)
+        got = out.cpu().numpy().reshape(o.size, p.dim, p.dim)
+        scale = max(1.0, float(np.max(np.abs(want))))
+        assert np.max(np.abs(got - want)) <= RHS_TOL * scale
+    o.close()
+
+
+def test_rhs_noalloc_rejects_misaligned_and_overlapping_buffers():
+    import torch
+
+    p = S.spin_glass(3, seed=7, depth=2, K=1, h=0.6)
+    n = capi.hierarchy_size(6, p.max_depth) * p.dim * p.dim
+    buf = torch.zeros(2 * n + 1, dtype=torch.complex128, device="cuda")
+    base = buf.data_ptr()
+    with pytest.raises(capi.HxError) as err:
+        capi.rhs_noalloc(p, base + 8, base + 16 * (n + 1), 0)
+    assert "16-byte aligned" in str(err.value)
+    with pytest.raises(capi.HxError) as err:
+        capi.rhs_noalloc(p, base, base + 16 * (n // 2), 0)
+    assert "overlap" in str(err.value)
