@@ -44,8 +44,8 @@ CONFIGS = {
                workload="spin_glass_d256_L3_K1_969ados_complex64_mixed"),
     # learned closure: N=5 (d=32), K=2 (15 modes), L=2 + MLP closure of tier 3; trained on 64 seeds of plain
     # L=5 FP64 runs (dt=0.01, 1000 steps), tested on 16 held-out seeds against plain L=5
-    "c5": dict(n=5, K=2, h=1.0, dt=0.01, closure=True, coarse_depth=2, fine_depth=5, train_seeds=16,
-               test_seeds=16, traj_steps=1000, every=50, hidden=128, iters=3000, mlp_batch=8192, lr=3e-3,
+    "c5": dict(n=5, K=2, h=1.0, dt=0.01, closure=True, coarse_depth=2, fine_depth=5, train_seeds=64,
+               test_seeds=16, traj_steps=1000, every=50, hidden=512, iters=3000, mlp_batch=8192, lr=3e-3,
                time_seeds=4, time_steps=250,
                workload="spin_glass_d32_K2_L2_plus_mlp_closure_vs_L5"),
     # batched disorder average: 512 seeded instances, N in {3,4,5}, L in {2,3,4}, K=2, dt=0.01
@@ -445,6 +445,8 @@ def run_ours(args, cfg: dict) -> None:
     # window
     windows = [window()]
     reps = max(MIN_WINDOWS, min(MAX_WINDOWS, int(np.ceil(WINDOW_TARGET_MS / max(windows[0], 1e-3)))))
+    if args.windows:
+        reps = args.windows
     if world > 1:
         t = torch.tensor([reps], device="cuda")
         dist.broadcast(t, 0)
@@ -969,6 +971,8 @@ def main() -> None:
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--windows", type=int, default=0,
+                    help="timed windows of --steps steps (default: repeat until ~1 s of device time, at least 5)")
     ap.add_argument("--no-ref-cuda", action="store_true",
                     help="skip timing the reference's own CUDA propagator at the workload's shape")
     args = ap.parse_args()

@@ -128,3 +128,27 @@ def test_packed_band_kernels_d256_and_d512_match_oracle():
             rho, en = ctx.step_trace(3)
         assert np.max(np.abs(rho - rho_ref)) < TOL
         assert np.max(np.abs(en - en_ref)) < TOL
+
+
+def test_mixed_precision_at_the_c3_shape():
+    """The C3 workload itself (N = 8, d = 256, K = 1: 16 modes, L = 3: 969
+    ADOs, h = 0.5, dt = 0.005): complex64 hierarchy with rho_0 in FP64 against
+    the FP64 propagator over 200 steps, trace distance of rho_0 <= 1e-6 every
+    10 steps, energy within 1e-6; the FP64 run's first steps against the oracle."""
+    p = S.spin_glass(8, seed=2027, depth=3, K=1, h=0.5, dt=0.005)
+    steps = 200
+    with capi.Context(p) as c64:
+        assert c64.size == 969
+        r64, e64 = c64.step_trace(steps)
+    with capi.Context(p, precision="mixed") as cm:
+        rm, em = cm.step_trace(steps)
+    td = [_trace_distance(rm[t], r64[t]) for t in range(9, steps, 10)]
+    assert max(td) <= 1e-6, max(td)
+    assert np.max(np.abs(em - e64)) <= 1e-6
+    # the trajectory moves away from the initial state: the comparison is not vacuous
+    assert _trace_distance(r64[-1], S.initial_rho0(p.dim)) > 1e-3
+    o = O.Oracle(p)
+    ro, eo = o.run(2, trace=True)
+    o.close()
+    assert np.max(np.abs(r64[:2] - ro)) < TOL
+    assert np.max(np.abs(e64[:2] - eo)) < TOL

@@ -53,7 +53,8 @@ def test_rhs_noalloc_matches_context_rhs_two_calls_in_a_row():
 def test_rhs_noalloc_rejects_hierarchies_beyond_its_scratch():
     big = S.spin_glass(6, seed=1, depth=6, K=2)  # 18 modes, depth 6: tables far beyond 8 MiB
     with pytest.raises(capi.HxError) as err:
-        capi.rhs_noalloc(big, 1, 1, 0)  # rejected before any device access
+        # aligned, non-overlapping stand-in addresses: rejected for its size before any device access
+        capi.rhs_noalloc(big, 1 << 40, 1 << 42, 0)
     assert err.value.status == "UnsupportedHierarchy"
     assert "bytes of scratch" in str(err.value)
 
