@@ -57,7 +57,7 @@ void release(hx_ctx* c)
                     c->ent_wc, c->ent_wa, c->order_perm, c->ado_keep, c->up_slot, c->up_ado, c->up_cnt,
                     c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf, c->rho32, c->ua32, c->ub32,
                     c->U32, c->diag32, c->vdiag32, c->hflip32, c->diag_herm, c->vbit, c->csr_ptr, c->csr_col,
-                    c->csr_val};
+                    c->csr_val, c->pack_scale, c->pack_bad, c->ticket};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -114,6 +114,10 @@ hx::FusedArgs hx::fused_args_of(const hx_ctx* c)
     a.herm = c->herm ? 1 : 0;
     a.vbit = c->vbit;
     a.pauli = c->vbit ? 1 : 0;
+    a.hdiag = c->hdiag;
+    a.xi = c->xi;
+    a.ticket = c->ticket;
+    a.sms = c->sm_count;
     return a;
 }
 
@@ -281,6 +285,14 @@ int launch_stage_core(hx_ctx* c, const double2* u, const double2* rho, double2* 
         hx::launch_flip_stage(flip_args_of(c), u, c->Bbuf, rho, out, alpha, base, c->stream);
         return 2;
     }
+    if (c->use_herm64) {
+        int k = 0;
+        if (c->up_slots > 0) {
+            hx::launch_upterm(hx::upterm_args_of(c), u, c->U, c->stream);
+            ++k;
+        }
+        if (hx::launch_herm64(hx::fused_args_of(c), u, rho, out, alpha, base, c->stream)) return k + 1;
+    }
     if (c->use_fused) {
         int k = 0;
         if (c->up_slots > 0) {
@@ -339,6 +351,7 @@ int read_error_flag(hx_ctx* c)
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (flag != 0) {
         cudaMemsetAsync(c->error_flag, 0, sizeof(int), c->stream);
+        if (c->ticket) cudaMemsetAsync(c->ticket, 0, 2 * sizeof(int), c->stream);  // a kernel that gave up
         return fail(HX_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration budget");
     }
     return HX_OK;
@@ -872,13 +885,21 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
             bool all_pauli = true;
             for (int j = 0; j < J; ++j) all_pauli = all_pauli && (bits[j] = hx::pauli_spin(vd.data() + static_cast<size_t>(j) * d, c->d)) >= 0;
             if (rc == HX_OK && all_pauli && (rc = dev_alloc(c, &c->vbit, J)) == HX_OK) rc = upload(c, c->vbit, bits);
+            // d = 64 with sigma_z couplings: the persistent kernel of hx_herm64.cu,
+            // which gathers the up terms of tier L-1 itself (every up neighbour
+            // in the entry lists) unless HX_HERM64_UPTERM=1 keeps the up-term pass
+            const char* h64_env = std::getenv("HX_HERM64");
+            const bool want_h64 = fused_ok && c->herm && all_pauli && hx::herm64_supported(logd, M, J, 1) &&
+                                  h64_env && h64_env[0] == '1';
+            const char* h64_up_env = std::getenv("HX_HERM64_UPTERM");
+            const bool h64_inplace = want_h64 && !(h64_up_env && h64_up_env[0] == '1');
             hx::launch_entries(c->rows, c->edges, c->acoef, c->bcoef, c->bath_off, c->H, M, J,
-                               static_cast<int>(p->max_depth), c->ent_count, c->ent_slab, c->ent_bath, c->ent_wc,
-                               c->ent_wa, c->ado_keep, c->stream);
+                               static_cast<int>(p->max_depth) + (h64_inplace ? 1 : 0), c->ent_count, c->ent_slab,
+                               c->ent_bath, c->ent_wc, c->ent_wa, c->ado_keep, c->stream);
             rc = check_launch("fused-kernel setup");
             // tier L-1 slots: count them first, then size the per-slot tables and U
             int S = 0;
-            if (rc == HX_OK && p->max_depth >= 2) {
+            if (rc == HX_OK && p->max_depth >= 2 && !h64_inplace) {
                 int32_t *tmp_slab = nullptr, *tmp_bath = nullptr;
                 e = cudaMalloc(&tmp_slab, H * M * sizeof(int32_t));
                 if (e == cudaSuccess) e = cudaMalloc(&tmp_bath, H * M * sizeof(int32_t));
@@ -913,6 +934,13 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
             }
             c->up_slots = S;
             c->use_fused = (rc == HX_OK) && fused_ok;
+            c->use_herm64 = c->use_fused && want_h64 && hx::prepare_herm64();
+            if (c->use_fused && want_h64 && !c->use_herm64)
+                rc = fail(HX_ERR_CUDA, "could not raise the shared-memory limit of herm64_kernel");
+            if (c->use_herm64 && rc == HX_OK && (rc = dev_alloc(c, &c->ticket, 2)) == HX_OK) {
+                e = cudaMemsetAsync(c->ticket, 0, 2 * sizeof(int), c->stream);
+                if (e != cudaSuccess) rc = hx::cuda_fail(e, "ticket counters");
+            }
             // single-precision copies of the operators for the mixed band kernel
             if (rc == HX_OK && c->mixed) {
                 if ((rc = dev_alloc(c, &c->diag32, c->slab)) || (rc = dev_alloc(c, &c->vdiag32, static_cast<size_t>(J) * d)) ||
@@ -1156,24 +1184,58 @@ int hx_ctx_write_state(hx_ctx* c, const double* in, uint64_t n)
         HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
         return HX_OK;
     }
-    if (c->herm) {
+    // full slabs that fit in the two stage buffers (scratch between steps)
+    const long long per_buf =
+        c->herm ? static_cast<long long>(static_cast<size_t>(c->H) * c->slab_store / c->slab) : 0;
+    if (c->herm && 2 * per_buf < c->H) {
+        // a tiny hierarchy: pack on the host
         const size_t n = static_cast<size_t>(c->H) * c->slab_store;
         int rc = state_staging(c, n);
         if (rc != HX_OK) return rc;
         HX_CUDA_TRY(cudaStreamSynchronize(c->stream));  // the staging buffer may still feed an earlier copy
         double2* pk = c->state_pinned;
-        std::vector<char> ok(static_cast<size_t>(c->H), 1);
-        parallel_for(c->H, [&](long long k) {
-            ok[k] = pack_herm_host(in + 2 * static_cast<size_t>(k) * c->slab, c->logd, pk + k * c->slab_store);
-        });
         for (long long k = 0; k < c->H; ++k)
-            if (!ok[k])
+            if (!pack_herm_host(in + 2 * static_cast<size_t>(k) * c->slab, c->logd, pk + k * c->slab_store))
                 return fail(HX_ERR_INVALID_RUNTIME_OPTION,
                             "ADO " + std::to_string(k) +
                                 " is not Hermitian; this context keeps Hermitian-packed slabs (create it with "
                                 "HX_FLAG_FULL_STATE for general states)");
         HX_CUDA_TRY(cudaMemcpyAsync(c->rho, pk, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
         c->counters.h2d_bytes += n * sizeof(double2);
+        HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return HX_OK;
+    }
+    if (c->herm) {
+        // the full slabs go up into the two stage buffers, are checked for
+        // Hermiticity on the device and only then packed into rho, so a
+        // rejected state leaves the context's state as it was
+        int rc = HX_OK;
+        if (!c->pack_scale && ((rc = dev_alloc(c, &c->pack_scale, c->H)) || (rc = dev_alloc(c, &c->pack_bad, 1))))
+            return rc;
+        const long long n0 = std::min<long long>(per_buf, c->H), n1 = c->H - n0;
+        const long long part_first[2] = {0, n0}, part_cnt[2] = {n0, n1};
+        double2* bufs[2] = {c->ua, c->ub};
+        HX_CUDA_TRY(cudaMemsetAsync(c->pack_bad, 0x7f, sizeof(int), c->stream));
+        for (int b = 0; b < 2; ++b) {
+            if (part_cnt[b] == 0) continue;
+            HX_CUDA_TRY(cudaMemcpyAsync(bufs[b], in + 2 * static_cast<size_t>(part_first[b]) * c->slab,
+                                        static_cast<size_t>(part_cnt[b]) * c->slab * sizeof(double2),
+                                        cudaMemcpyHostToDevice, c->stream));
+            hx::launch_herm_check(bufs[b], part_cnt[b], c->logd, 1e-12, c->pack_scale, part_first[b], c->pack_bad,
+                                  c->stream);
+            c->counters.h2d_bytes += static_cast<size_t>(part_cnt[b]) * c->slab * sizeof(double2);
+        }
+        HX_CUDA_TRY(cudaGetLastError());
+        int bad = 0;
+        HX_CUDA_TRY(cudaMemcpyAsync(&bad, c->pack_bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (bad != 0x7f7f7f7f)
+            return fail(HX_ERR_INVALID_RUNTIME_OPTION,
+                        "ADO " + std::to_string(bad) +
+                            " is not Hermitian; this context keeps Hermitian-packed slabs (create it with "
+                            "HX_FLAG_FULL_STATE for general states)");
+        for (int b = 0; b < 2; ++b) hx::launch_herm_pack(bufs[b], part_cnt[b], c->logd, part_first[b], c->rho, c->stream);
+        HX_CUDA_TRY(cudaGetLastError());
         HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
         return HX_OK;
     }

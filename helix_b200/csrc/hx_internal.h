@@ -114,6 +114,12 @@ __host__ __device__ inline void herm_coords(int i, int logd, int& r, int& c)
 }
 // Packed copy of a full d x d table (upper triangle).
 void launch_pack_herm(const double2* full, int logd, double2* packed, cudaStream_t s);
+// count full slabs: the Hermiticity check of the host packer (relative to each slab's largest element; *bad
+// is lowered to the index first + k of a slab that fails it), then the packing into slabs first.. of `packed`
+void launch_herm_check(const double2* full, long long count, int logd, double rel_tol, double* scale2,
+                       long long first, int* bad, cudaStream_t s);
+void launch_herm_pack(const double2* full, long long count, int logd, long long first, double2* packed,
+                      cudaStream_t s);
 // Full row-major complex matrix (2 d^2 doubles) from a packed slab, on the host.
 void unpack_herm_host(const double2* pk, int logd, double* out);
 
@@ -142,8 +148,17 @@ struct FusedArgs {
     int herm;                // 1: slabs Hermitian-packed (herm_elems(logd) elements), diag and U packed too
     const int* vbit;         // [J] spin of V_j = sigma_z(spin) for every bath (pauli = 1), else nullptr
     int pauli;
+    const double* hdiag;     // [d] diagonal of H (E_r)
+    const double* xi;        // [J] low-temperature correction coefficients
+    int* ticket;             // [2] ADO ticket and finished-CTA counters of herm64_kernel (zero between launches)
+    int sms;                 // SMs of the device (grid of herm64_kernel)
 };
 bool fused_supported(int logd, int M, int J, int herm);
+// d = 64, packed slabs, sigma_z couplings: the persistent TMA-ring kernel (hx_herm64.cu)
+bool herm64_supported(int logd, int M, int J, int pauli);
+bool prepare_herm64();  // raises the shared-memory limit; call before stream capture
+bool launch_herm64(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
+                   int base_kind, cudaStream_t s);
 bool prepare_fused(int logd, int M, int J, int herm);  // raises the shared-memory limit; call before stream capture
 bool launch_fused(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
                   int base_kind, cudaStream_t s);
@@ -348,6 +363,8 @@ struct hx_ctx {
     int* error_flag = nullptr;
     // fused stage-kernel tables (d = 32, 64)
     bool use_fused = false;
+    bool use_herm64 = false;      // d = 64 packed sigma_z stage kernel (hx_herm64.cu)
+    int* ticket = nullptr;        // [2] counters of herm64_kernel
     int sm_count = 0;
     int up_slots = 0;             // ADOs in tier L-1
     int32_t* up_slot = nullptr;   // [H]
@@ -373,6 +390,8 @@ struct hx_ctx {
     double* pinned = nullptr;     // pinned staging for traces
     size_t pinned_bytes = 0;
     double2* state_pinned = nullptr; // pinned staging for packed whole-state transfers
+    double* pack_scale = nullptr;    // [H] per-slab scale of the device-side packer (first use)
+    int* pack_bad = nullptr;         // first ADO that failed the packer's Hermiticity check
     size_t state_pinned_elems = 0;
     size_t device_bytes = 0;
     hx_counters counters{};

@@ -307,7 +307,72 @@ __global__ void pack_herm_kernel(const double2* __restrict__ full, int logd, dou
     packed[i] = full[(r << logd) + c];
 }
 
+// scale2[k] = max |x|^2 over full slab k (one block per slab).
+__global__ void slab_max_kernel(const double2* __restrict__ full, long long slab, double* __restrict__ scale2)
+{
+    __shared__ double red[256];
+    const double2* x = full + blockIdx.x * slab;
+    double m = 0.0;
+    for (long long e = threadIdx.x; e < slab; e += blockDim.x) {
+        const double2 v = x[e];
+        m = fmax(m, v.x * v.x + v.y * v.y);
+    }
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) scale2[blockIdx.x] = red[0];
+}
+
+// Check (packed == nullptr) or pack `count` full slabs into Hermitian-packed
+// slabs first .. first + count - 1 of `packed`.  The check lowers *bad to the
+// index of an ADO whose (c, r) differs from conj (r, c) by more than
+// sqrt(rel_tol2 * scale2).
+__global__ void pack_check_kernel(const double2* __restrict__ full, long long count, int logd, double rel_tol2,
+                                  const double* __restrict__ scale2, long long first, double2* __restrict__ packed,
+                                  int* bad)
+{
+    const int D = 1 << logd;
+    const long long P = herm_elems(logd);
+    const long long total = count * P;
+    for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long k = t / P;
+        const int i = static_cast<int>(t - k * P);
+        int r, c;
+        herm_coords(i, logd, r, c);
+        const double2* x = full + k * static_cast<long long>(D) * D;
+        const double2 up = x[static_cast<long long>(r) * D + c];
+        if (!packed) {
+            if (r != c) {
+                const double2 lo = x[static_cast<long long>(c) * D + r];
+                const double dr = up.x - lo.x, di = up.y + lo.y;
+                if (dr * dr + di * di > rel_tol2 * scale2[k]) atomicMin(bad, static_cast<int>(first + k));
+            }
+        } else {
+            packed[(first + k) * P + i] = up;
+        }
+    }
+}
+
 }  // namespace
+
+void launch_herm_check(const double2* full, long long count, int logd, double rel_tol, double* scale2,
+                       long long first, int* bad, cudaStream_t s)
+{
+    if (count <= 0) return;
+    slab_max_kernel<<<static_cast<unsigned>(count), 256, 0, s>>>(full, 1LL << (2 * logd), scale2);
+    pack_check_kernel<<<148 * 8, 256, 0, s>>>(full, count, logd, rel_tol * rel_tol, scale2, first, nullptr, bad);
+}
+
+void launch_herm_pack(const double2* full, long long count, int logd, long long first, double2* packed,
+                      cudaStream_t s)
+{
+    if (count <= 0) return;
+    pack_check_kernel<<<148 * 8, 256, 0, s>>>(full, count, logd, 0.0, nullptr, first, packed, nullptr);
+}
 
 void launch_stage(const StageTables& t, const double2* u, const double2* rho, double2* out, double alpha,
                   int base_kind, cudaStream_t s)
