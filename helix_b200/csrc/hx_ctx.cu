@@ -285,6 +285,7 @@ int launch_stage_core(hx_ctx* c, const double2* u, const double2* rho, double2* 
         hx::launch_flip_stage(flip_args_of(c), u, c->Bbuf, rho, out, alpha, base, c->stream);
         return 2;
     }
+    if (c->use_small && hx::launch_small(hx::fused_args_of(c), u, rho, out, alpha, base, c->stream)) return 1;
     if (c->use_herm64) {
         int k = 0;
         if (c->up_slots > 0) {
@@ -760,6 +761,11 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     const bool fused_ok = !c->use_flip && !c->use_large && !c->use_csr && logd >= 5 && logd <= hx::kMaxLogD &&
                           hx::fused_supported(logd, M, J, want_herm ? 1 : 0) &&
                           !(force_generic && force_generic[0] == '1');
+    // small slabs (d <= 16) with sigma_z couplings: batched-gather kernel (hx_small.cu)
+    const char* small_env = std::getenv("HX_SMALL_STAGE");
+    const bool small_ok = !c->use_flip && !c->use_large && !c->use_csr && logd <= 4 &&
+                          hx::small_supported(logd, M, 1) && !(force_generic && force_generic[0] == '1') &&
+                          small_env && small_env[0] == '1';
     c->herm = (fused_ok || c->use_large) && want_herm;
     c->slab_store = c->herm ? static_cast<size_t>(hx::herm_elems(logd)) : c->slab;
     const size_t nstate = static_cast<size_t>(H) * c->slab_store;
@@ -868,7 +874,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
         rc = check_launch("setup kernels");
     }
     // fused stage kernel (d = 32, 64): neighbour entry lists, diagonal table, up-term tables
-    if (rc == HX_OK && (fused_ok || c->use_large)) {
+    if (rc == HX_OK && (fused_ok || c->use_large || small_ok)) {
         cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
         int* dS = nullptr;
         if ((rc = dev_alloc(c, &c->diag_table, c->slab)) || (rc = dev_alloc(c, &c->ent_count, H)) ||
@@ -893,13 +899,15 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                                   h64_env && h64_env[0] == '1';
             const char* h64_up_env = std::getenv("HX_HERM64_UPTERM");
             const bool h64_inplace = want_h64 && !(h64_up_env && h64_up_env[0] == '1');
+            const bool want_small = small_ok && all_pauli;
             hx::launch_entries(c->rows, c->edges, c->acoef, c->bcoef, c->bath_off, c->H, M, J,
-                               static_cast<int>(p->max_depth) + (h64_inplace ? 1 : 0), c->ent_count, c->ent_slab,
+                               static_cast<int>(p->max_depth) + (h64_inplace || want_small ? 1 : 0), c->ent_count,
+                               c->ent_slab,
                                c->ent_bath, c->ent_wc, c->ent_wa, c->ado_keep, c->stream);
             rc = check_launch("fused-kernel setup");
             // tier L-1 slots: count them first, then size the per-slot tables and U
             int S = 0;
-            if (rc == HX_OK && p->max_depth >= 2 && !h64_inplace) {
+            if (rc == HX_OK && p->max_depth >= 2 && !h64_inplace && !small_ok) {
                 int32_t *tmp_slab = nullptr, *tmp_bath = nullptr;
                 e = cudaMalloc(&tmp_slab, H * M * sizeof(int32_t));
                 if (e == cudaSuccess) e = cudaMalloc(&tmp_bath, H * M * sizeof(int32_t));
@@ -934,6 +942,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
             }
             c->up_slots = S;
             c->use_fused = (rc == HX_OK) && fused_ok;
+            c->use_small = (rc == HX_OK) && want_small;
             c->use_herm64 = c->use_fused && want_h64 && hx::prepare_herm64();
             if (c->use_fused && want_h64 && !c->use_herm64)
                 rc = fail(HX_ERR_CUDA, "could not raise the shared-memory limit of herm64_kernel");

@@ -154,6 +154,11 @@ struct FusedArgs {
     int sms;                 // SMs of the device (grid of herm64_kernel)
 };
 bool fused_supported(int logd, int M, int J, int herm);
+// d <= 16, full slabs, sigma_z couplings, every up term in the entry lists: batched gathers (hx_small.cu)
+size_t small_smem(int logd, int M);
+bool small_supported(int logd, int M, int pauli);
+bool launch_small(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
+                  int base_kind, cudaStream_t s);
 // d = 64, packed slabs, sigma_z couplings: the persistent TMA-ring kernel (hx_herm64.cu)
 bool herm64_supported(int logd, int M, int J, int pauli);
 bool prepare_herm64();  // raises the shared-memory limit; call before stream capture
@@ -364,6 +369,7 @@ struct hx_ctx {
     // fused stage-kernel tables (d = 32, 64)
     bool use_fused = false;
     bool use_herm64 = false;      // d = 64 packed sigma_z stage kernel (hx_herm64.cu)
+    bool use_small = false;       // d <= 16 sigma_z stage kernel (hx_small.cu)
     int* ticket = nullptr;        // [2] counters of herm64_kernel
     int sm_count = 0;
     int up_slots = 0;             // ADOs in tier L-1
