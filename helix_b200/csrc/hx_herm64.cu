@@ -166,7 +166,9 @@ __device__ __forceinline__ bool consumers_any(bool v)
     return r != 0;
 }
 
-__global__ void __maxnreg__(112)
+// 18 warps: the busiest of the four SM sub-partitions holds 5 of them, and its
+// 16K registers cap a thread at 96.
+__global__ void __launch_bounds__(kThreads, 1)
     herm64_kernel(FusedArgs a, const double2* __restrict__ u, const double2* rho, double2* out, double alpha,
                   int base_kind)
 {
@@ -443,6 +445,10 @@ bool prepare_herm64()
     if (configured[dev] == 0) {
         if (cudaFuncSetAttribute(herm64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(herm64_smem())) != cudaSuccess)
+            return false;
+        // the block must fit one SM (registers and shared memory)
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, herm64_kernel) != cudaSuccess || fa.maxThreadsPerBlock < kThreads)
             return false;
         configured[dev] = herm64_smem();
     }
