@@ -238,6 +238,8 @@ def stage_kernels_label(ctx, p, packed: bool, per_stage: int) -> str:
         k = f"herm_kernel<{logd}>" if packed else f"fused_kernel<{logd}>"
         return k + (" + upterm_kernel" if per_stage == 2 else "") + " per stage" + \
             (" (Hermitian-packed slabs)" if packed else "")
+    if path == "small":
+        return "small_kernel per stage (d <= 16, batched neighbour gathers)"
     return "stage_kernel per stage (generic path)"
 
 

@@ -88,7 +88,7 @@ class Info(C.Structure):
 
 
 # hx_info.stage_path (HX_PATH_*)
-STAGE_PATHS = {0: "generic", 1: "fused", 2: "band", 3: "flip", 4: "csr"}
+STAGE_PATHS = {0: "generic", 1: "fused", 2: "band", 3: "flip", 4: "csr", 5: "small"}
 
 
 class Counters(C.Structure):

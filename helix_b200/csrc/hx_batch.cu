@@ -816,8 +816,7 @@ void launch_batch_stage(hx_batch* b, int in_id, int out_id, double alpha, int ba
         cudaStream_t sg = g == 0 ? s : b->gstream[g];
         double2* cb[3] = {c->rho, c->ua, c->ub};
         if (c->up_slots > 0) hx::launch_upterm(hx::upterm_args_of(c), cb[in_id], c->U, sg);
-        if (!(c->use_herm64 && hx::launch_herm64(b->fargs[k], cb[in_id], c->rho, cb[out_id], alpha, base, sg)))
-            hx::launch_fused(b->fargs[k], cb[in_id], c->rho, cb[out_id], alpha, base, sg);
+        hx::launch_fused(b->fargs[k], cb[in_id], c->rho, cb[out_id], alpha, base, sg);
     }
     for (int g = 1; g < b->ngroups; ++g) {
         cudaEventRecord(b->ev_join[g], b->gstream[g]);

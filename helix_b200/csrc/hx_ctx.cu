@@ -57,7 +57,7 @@ void release(hx_ctx* c)
                     c->ent_wc, c->ent_wa, c->order_perm, c->ado_keep, c->up_slot, c->up_ado, c->up_cnt,
                     c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf, c->rho32, c->ua32, c->ub32,
                     c->U32, c->diag32, c->vdiag32, c->hflip32, c->diag_herm, c->vbit, c->csr_ptr, c->csr_col,
-                    c->csr_val, c->pack_scale, c->pack_bad, c->ticket};
+                    c->csr_val, c->pack_scale, c->pack_bad};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -116,8 +116,6 @@ hx::FusedArgs hx::fused_args_of(const hx_ctx* c)
     a.pauli = c->vbit ? 1 : 0;
     a.hdiag = c->hdiag;
     a.xi = c->xi;
-    a.ticket = c->ticket;
-    a.sms = c->sm_count;
     return a;
 }
 
@@ -286,14 +284,6 @@ int launch_stage_core(hx_ctx* c, const double2* u, const double2* rho, double2* 
         return 2;
     }
     if (c->use_small && hx::launch_small(hx::fused_args_of(c), u, rho, out, alpha, base, c->stream)) return 1;
-    if (c->use_herm64) {
-        int k = 0;
-        if (c->up_slots > 0) {
-            hx::launch_upterm(hx::upterm_args_of(c), u, c->U, c->stream);
-            ++k;
-        }
-        if (hx::launch_herm64(hx::fused_args_of(c), u, rho, out, alpha, base, c->stream)) return k + 1;
-    }
     if (c->use_fused) {
         int k = 0;
         if (c->up_slots > 0) {
@@ -352,7 +342,6 @@ int read_error_flag(hx_ctx* c)
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (flag != 0) {
         cudaMemsetAsync(c->error_flag, 0, sizeof(int), c->stream);
-        if (c->ticket) cudaMemsetAsync(c->ticket, 0, 2 * sizeof(int), c->stream);  // a kernel that gave up
         return fail(HX_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration budget");
     }
     return HX_OK;
@@ -765,7 +754,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     const char* small_env = std::getenv("HX_SMALL_STAGE");
     const bool small_ok = !c->use_flip && !c->use_large && !c->use_csr && logd <= 4 &&
                           hx::small_supported(logd, M, 1) && !(force_generic && force_generic[0] == '1') &&
-                          small_env && small_env[0] == '1';
+                          !(small_env && small_env[0] == '0');
     c->herm = (fused_ok || c->use_large) && want_herm;
     c->slab_store = c->herm ? static_cast<size_t>(hx::herm_elems(logd)) : c->slab;
     const size_t nstate = static_cast<size_t>(H) * c->slab_store;
@@ -891,23 +880,16 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
             bool all_pauli = true;
             for (int j = 0; j < J; ++j) all_pauli = all_pauli && (bits[j] = hx::pauli_spin(vd.data() + static_cast<size_t>(j) * d, c->d)) >= 0;
             if (rc == HX_OK && all_pauli && (rc = dev_alloc(c, &c->vbit, J)) == HX_OK) rc = upload(c, c->vbit, bits);
-            // d = 64 with sigma_z couplings: the persistent kernel of hx_herm64.cu,
-            // which gathers the up terms of tier L-1 itself (every up neighbour
-            // in the entry lists) unless HX_HERM64_UPTERM=1 keeps the up-term pass
-            const char* h64_env = std::getenv("HX_HERM64");
-            const bool want_h64 = fused_ok && c->herm && all_pauli && hx::herm64_supported(logd, M, J, 1) &&
-                                  h64_env && h64_env[0] == '1';
-            const char* h64_up_env = std::getenv("HX_HERM64_UPTERM");
-            const bool h64_inplace = want_h64 && !(h64_up_env && h64_up_env[0] == '1');
+            // small slabs: every up neighbour in the entry lists (no up-term pass)
             const bool want_small = small_ok && all_pauli;
             hx::launch_entries(c->rows, c->edges, c->acoef, c->bcoef, c->bath_off, c->H, M, J,
-                               static_cast<int>(p->max_depth) + (h64_inplace || want_small ? 1 : 0), c->ent_count,
+                               static_cast<int>(p->max_depth) + (want_small ? 1 : 0), c->ent_count,
                                c->ent_slab,
                                c->ent_bath, c->ent_wc, c->ent_wa, c->ado_keep, c->stream);
             rc = check_launch("fused-kernel setup");
             // tier L-1 slots: count them first, then size the per-slot tables and U
             int S = 0;
-            if (rc == HX_OK && p->max_depth >= 2 && !h64_inplace && !small_ok) {
+            if (rc == HX_OK && p->max_depth >= 2 && !small_ok) {
                 int32_t *tmp_slab = nullptr, *tmp_bath = nullptr;
                 e = cudaMalloc(&tmp_slab, H * M * sizeof(int32_t));
                 if (e == cudaSuccess) e = cudaMalloc(&tmp_bath, H * M * sizeof(int32_t));
@@ -943,13 +925,6 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
             c->up_slots = S;
             c->use_fused = (rc == HX_OK) && fused_ok;
             c->use_small = (rc == HX_OK) && want_small;
-            c->use_herm64 = c->use_fused && want_h64 && hx::prepare_herm64();
-            if (c->use_fused && want_h64 && !c->use_herm64)
-                rc = fail(HX_ERR_CUDA, "could not raise the shared-memory limit of herm64_kernel");
-            if (c->use_herm64 && rc == HX_OK && (rc = dev_alloc(c, &c->ticket, 2)) == HX_OK) {
-                e = cudaMemsetAsync(c->ticket, 0, 2 * sizeof(int), c->stream);
-                if (e != cudaSuccess) rc = hx::cuda_fail(e, "ticket counters");
-            }
             // single-precision copies of the operators for the mixed band kernel
             if (rc == HX_OK && c->mixed) {
                 if ((rc = dev_alloc(c, &c->diag32, c->slab)) || (rc = dev_alloc(c, &c->vdiag32, static_cast<size_t>(J) * d)) ||
@@ -1022,6 +997,7 @@ int hx_ctx_info(const hx_ctx* c, hx_info* info)
                        : c->use_flip ? HX_PATH_FLIP
                        : c->use_large ? HX_PATH_BAND
                        : c->use_fused ? HX_PATH_FUSED
+                       : c->use_small ? HX_PATH_SMALL
                        : HX_PATH_GENERIC;
     return HX_OK;
 }

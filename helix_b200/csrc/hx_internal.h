@@ -150,8 +150,6 @@ struct FusedArgs {
     int pauli;
     const double* hdiag;     // [d] diagonal of H (E_r)
     const double* xi;        // [J] low-temperature correction coefficients
-    int* ticket;             // [2] ADO ticket and finished-CTA counters of herm64_kernel (zero between launches)
-    int sms;                 // SMs of the device (grid of herm64_kernel)
 };
 bool fused_supported(int logd, int M, int J, int herm);
 // d <= 16, full slabs, sigma_z couplings, every up term in the entry lists: batched gathers (hx_small.cu)
@@ -159,11 +157,6 @@ size_t small_smem(int logd, int M);
 bool small_supported(int logd, int M, int pauli);
 bool launch_small(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
                   int base_kind, cudaStream_t s);
-// d = 64, packed slabs, sigma_z couplings: the persistent TMA-ring kernel (hx_herm64.cu)
-bool herm64_supported(int logd, int M, int J, int pauli);
-bool prepare_herm64();  // raises the shared-memory limit; call before stream capture
-bool launch_herm64(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
-                   int base_kind, cudaStream_t s);
 bool prepare_fused(int logd, int M, int J, int herm);  // raises the shared-memory limit; call before stream capture
 bool launch_fused(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
                   int base_kind, cudaStream_t s);
@@ -368,9 +361,7 @@ struct hx_ctx {
     int* error_flag = nullptr;
     // fused stage-kernel tables (d = 32, 64)
     bool use_fused = false;
-    bool use_herm64 = false;      // d = 64 packed sigma_z stage kernel (hx_herm64.cu)
     bool use_small = false;       // d <= 16 sigma_z stage kernel (hx_small.cu)
-    int* ticket = nullptr;        // [2] counters of herm64_kernel
     int sm_count = 0;
     int up_slots = 0;             // ADOs in tier L-1
     int32_t* up_slot = nullptr;   // [H]

@@ -134,6 +134,7 @@ typedef struct hx_info {
 #define HX_PATH_BAND 2u     /* band kernels: 128 <= d <= 1024, diagonal couplings */
 #define HX_PATH_FLIP 3u     /* comm_kernel + combine_kernel: couplings with spin flips */
 #define HX_PATH_CSR 4u      /* csr_comm_kernel + csr_combine_kernel: general sparse operators */
+#define HX_PATH_SMALL 5u    /* small_kernel: d <= 16 with sigma_z couplings (batched neighbour gathers) */
 
 /* Profiling counters (replaces src/library/backend_profiling.cpp:9-137). */
 typedef struct hx_counters {

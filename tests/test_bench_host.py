@@ -71,6 +71,7 @@ class _Ctx:
     ("flip", False, 2, "comm_kernel + combine_kernel per stage (spin-flip coupling path)"),
     ("csr", False, 2, "csr_comm_kernel + csr_combine_kernel per stage (general sparse operators)"),
     ("generic", False, 1, "stage_kernel per stage (generic path)"),
+    ("small", False, 1, "small_kernel per stage (d <= 16, batched neighbour gathers)"),
 ])
 def test_stage_kernel_labels(path, packed, per_stage, want):
     p = S.spin_glass(6, seed=1, depth=1, K=1)

@@ -1,12 +1,8 @@
-"""The specialised stage kernels against the oracle, each selected explicitly:
-
-* hx_small.cu (d <= 16, sigma_z couplings, batched neighbour gathers);
-* hx_herm64.cu (d = 64, packed slabs, sigma_z couplings, persistent kernel
-  fed by a TMA ring), with the up terms of tier L-1 gathered in the kernel
-  and with the separate up-term pass.
-
-RHS within 1e-12 relative and trajectories within 1e-10 max-abs, the
-tolerances of the other parity tests."""
+"""The small-slab stage kernels against the oracle: small_kernel (hx_small.cu,
+d <= 16 with sigma_z couplings, batched neighbour gathers; the default for
+those shapes) and the generic stage_kernel it replaces there
+(HX_SMALL_STAGE=0).  RHS within 1e-12 relative and trajectories within 1e-10
+max-abs, the tolerances of the other parity tests."""
 import numpy as np
 import pytest
 
@@ -20,15 +16,10 @@ TOL = 1e-10
 RHS_TOL = 1e-12
 
 
-def _hermitian_state(size, d, seed):
-    rng = np.random.default_rng(seed)
-    x = rng.standard_normal((size, d, d)) + 1j * rng.standard_normal((size, d, d))
-    return 0.5 * (x + np.conj(np.transpose(x, (0, 2, 1))))
-
-
+@pytest.mark.parametrize("path", ["small", "generic"])
 @pytest.mark.parametrize("n", [1, 2, 3, 4])
-def test_small_kernel_rhs(monkeypatch, n):
-    monkeypatch.setenv("HX_SMALL_STAGE", "1")
+def test_small_slab_rhs(monkeypatch, n, path):
+    monkeypatch.setenv("HX_SMALL_STAGE", "1" if path == "small" else "0")
     p = S.spin_glass(n, seed=40 + n, depth=3, K=2, h=0.8)
     o = O.Oracle(p)
     rng = np.random.default_rng(n)
@@ -36,6 +27,7 @@ def test_small_kernel_rhs(monkeypatch, n):
     want = o.rhs(x)
     o.close()
     with capi.Context(p) as ctx:
+        assert ctx.stage_path == path
         ctx.set_state(x)
         got = ctx.rhs()
     assert np.max(np.abs(got - want)) <= RHS_TOL * max(1.0, np.max(np.abs(want)))
@@ -50,37 +42,7 @@ def test_small_kernel_c1_trajectory(monkeypatch):
     rho_ref, en_ref = o.run(steps, trace=True)
     o.close()
     with capi.Context(p) as ctx:
-        assert ctx.size == 455
+        assert ctx.size == 455 and ctx.stage_path == "small"
         rho, en = ctx.step_trace(steps)
     assert np.max(np.abs(rho - rho_ref)) <= TOL
     assert np.max(np.abs(en - en_ref)) <= TOL
-
-
-@pytest.mark.parametrize("upterm", ["0", "1"])
-def test_herm64_rhs_and_trajectory(monkeypatch, upterm):
-    """d = 64, 12 modes, L = 2 and L = 3: the RHS of a random Hermitian state
-    populating every tier, then 20 steps from the reference initial state."""
-    monkeypatch.setenv("HX_HERM64", "1")
-    monkeypatch.setenv("HX_HERM64_UPTERM", upterm)
-    for depth in (2, 3):
-        p = S.spin_glass(6, seed=60 + depth, depth=depth, K=1, h=0.7, dt=0.005)
-        o = O.Oracle(p)
-        x = _hermitian_state(o.size, p.dim, depth) * 1e-2
-        want = o.rhs(x)
-        with capi.Context(p) as ctx:
-            assert ctx.hermitian_packed
-            ctx.set_state(x)
-            got = ctx.rhs()
-            assert np.max(np.abs(got - want)) <= RHS_TOL * max(1.0, np.max(np.abs(want)))
-            x0 = np.concatenate([S.initial_rho0(p.dim)[None], np.zeros((ctx.size - 1, p.dim, p.dim))])
-            ctx.set_state(x0)
-            o.set_state(x0)
-            rho, en = ctx.step_trace(20)
-            st = ctx.state()
-        rho_ref, en_ref = o.run(20, trace=True)
-        assert np.max(np.abs(rho - rho_ref)) <= TOL
-        assert np.max(np.abs(en - en_ref)) <= TOL
-        assert np.max(np.abs(st - o.state())) <= TOL
-        # the diagonal of every ADO stays exactly real
-        assert np.all(np.einsum("nii->ni", st).imag == 0.0)
-        o.close()
