@@ -23,7 +23,7 @@ LIB = os.path.join(OUT, "libhelix_b200.so")
 CXX_LIB = os.path.join(OUT, "libhelix.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["hx_host.cpp", "hx_tables.cu", "hx_stage.cu", "hx_fused.cu", "hx_small.cu", "hx_upterm.cu", "hx_flip.cu", "hx_csr.cu", "hx_large.cu", "hx_mlp.cu", "hx_ctx.cu", "hx_batch.cu", "hx_noalloc.cu"]
+CUDA_SOURCES = ["hx_host.cpp", "hx_tables.cu", "hx_stage.cu", "hx_fused.cu", "hx_small.cu", "hx_upterm.cu", "hx_flip.cu", "hx_csr.cu", "hx_large.cu", "hx_tcgemm.cu", "hx_mlp.cu", "hx_ctx.cu", "hx_batch.cu", "hx_noalloc.cu"]
 CXX_SOURCES = ["helix_api.cpp"]
 
 

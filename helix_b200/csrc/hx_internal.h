@@ -152,6 +152,22 @@ struct FusedArgs {
     const double* xi;        // [J] low-temperature correction coefficients
 };
 bool fused_supported(int logd, int M, int J, int herm);
+// BF16 GEMM on the tensor cores (hx_tcgemm.cu): C = A B^T, A [M x K] and B [N x K] row-major, FP32
+// accumulation, with the closure network's epilogues.  Returns false (nothing launched) when the operands
+// do not suit the tensor loads (16-byte aligned bases, leading dimensions multiples of 8).
+enum TcEpi : int { kTcEpiBiasGelu = 0, kTcEpiBias = 1, kTcEpiStore = 2, kTcEpiGeluBack = 3 };
+struct TcGemmOut {
+    int kind;           // TcEpi
+    const float* bias;  // [N]
+    float* outf;        // FP32 result (the pre-activation for kTcEpiBiasGelu)
+    void* outh;         // BF16 result (the GELU output, or dZ for kTcEpiGeluBack)
+    const float* aux;   // pre-activation Z for kTcEpiGeluBack
+    int ldo;
+};
+bool tc_gemm_eligible(const void* A, int lda, const void* B, int ldb);
+bool tc_gemm(int M, int N, int K, const void* A, int lda, const void* B, int ldb, const TcGemmOut& o, int* err,
+             cudaStream_t s);
+void launch_transpose_bf16(const void* in, int rows, int cols, int ld_in, void* out, int ld_out, cudaStream_t s);
 // d <= 16, full slabs, sigma_z couplings, every up term in the entry lists: batched gathers (hx_small.cu)
 size_t small_smem(int logd, int M);
 bool small_supported(int logd, int M, int pauli);

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -153,9 +154,53 @@ __global__ void __launch_bounds__(GT)
     }
 }
 
-template <bool TA, bool TB, int EPI>
-void gemm(int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb, const GemmOut& o, cudaStream_t s)
+// Scratch of the tensor-core path: K-major copies of operands stored the other
+// way round (hx_tcgemm.cu computes A B^T with both K-major), and its error word.
+struct TcScratch {
+    bf16* a = nullptr;
+    bf16* b = nullptr;
+    size_t a_elems = 0, b_elems = 0;
+    int* err = nullptr;
+};
+
+bool tc_enabled()
 {
+    static const bool v = [] {
+        const char* e = std::getenv("HX_TC_GEMM");
+        return e && e[0] == '1';
+    }();
+    return v;
+}
+
+inline int round8(int x) { return (x + 7) & ~7; }
+
+// C[M x N] = op(A) op(B): on the tensor cores (tcgen05, hx_tcgemm.cu) when the
+// operands allow it, the transposed layouts first copied K-major into the
+// scratch; otherwise the WMMA kernel above.
+template <bool TA, bool TB, int EPI>
+void gemm(int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb, const GemmOut& o, cudaStream_t s,
+          TcScratch* ts = nullptr)
+{
+    if (ts && tc_enabled()) {
+        const bf16* a = A;
+        const bf16* b = B;
+        int la = lda, lb = ldb;
+        bool ok = true;
+        if (TA) {  // A stored K x M
+            la = round8(K);
+            ok = ok && static_cast<size_t>(M) * la <= ts->a_elems;
+            if (ok) launch_transpose_bf16(A, K, M, lda, ts->a, la, s);
+            a = ts->a;
+        }
+        if (!TB) {  // B stored K x N
+            lb = round8(K);
+            ok = ok && static_cast<size_t>(N) * lb <= ts->b_elems;
+            if (ok) launch_transpose_bf16(B, K, N, ldb, ts->b, lb, s);
+            b = ts->b;
+        }
+        const TcGemmOut to{EPI, o.bias, o.outf, o.outh, o.aux, o.ldo};
+        if (ok && tc_gemm(M, N, K, a, la, b, lb, to, ts->err, s)) return;
+    }
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
     gemm_kernel<TA, TB, EPI><<<grid, GT, 0, s>>>(M, N, K, A, lda, B, ldb, o);
 }
@@ -471,15 +516,20 @@ struct hx_mlp {
     float* pinned = nullptr;
     // parameter offsets
     long long oW1 = 0, ob1 = 0, oW2 = 0, ob2 = 0, oW3 = 0, ob3 = 0;
+    // tensor-core GEMM scratch (transposed operands) and error word
+    hx::TcScratch tc;
 };
 
 namespace {
 
 void mlp_free_batch(hx_mlp* n)
 {
-    void* p[] = {n->X, n->H1, n->H2, n->dYh, n->dZ2h, n->dZ1h, n->Z1, n->Z2, n->Y, n->T, n->dYf, n->dZ2f, n->dZ1f};
+    void* p[] = {n->X, n->H1, n->H2, n->dYh, n->dZ2h, n->dZ1h, n->Z1, n->Z2, n->Y, n->T, n->dYf, n->dZ2f, n->dZ1f,
+                 n->tc.a, n->tc.b};
     for (void* q : p)
         if (q) cudaFree(q);
+    n->tc.a = n->tc.b = nullptr;
+    n->tc.a_elems = n->tc.b_elems = 0;
     n->X = n->H1 = n->H2 = n->dYh = n->dZ2h = n->dZ1h = nullptr;
     n->Z1 = n->Z2 = n->Y = n->T = n->dYf = n->dZ2f = n->dZ1f = nullptr;
     n->cap = 0;
@@ -503,6 +553,12 @@ int mlp_reserve(hx_mlp* n, int batch)
     if (e == cudaSuccess) e = cudaMalloc(&n->dYf, B * n->out_dim * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&n->dZ2f, B * n->hidden * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&n->dZ1f, B * n->hidden * sizeof(float));
+    // transposed operands: rows up to max(hidden, out, in), leading dimension up to max(batch, hidden, out) rounded to 8
+    const size_t rows = static_cast<size_t>(std::max(n->hidden, std::max(n->out_dim, n->in_ld)));
+    const size_t cols = static_cast<size_t>((std::max(batch, std::max(n->hidden, n->out_dim)) + 7) & ~7);
+    if (e == cudaSuccess) e = cudaMalloc(&n->tc.a, rows * cols * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc(&n->tc.b, rows * cols * sizeof(bf16));
+    if (e == cudaSuccess) n->tc.a_elems = n->tc.b_elems = rows * cols;
     if (e != cudaSuccess) {
         mlp_free_batch(n);
         return hx::cuda_fail(e, "cudaMalloc (MLP activations)");
@@ -517,11 +573,11 @@ void mlp_forward(hx_mlp* n, int B, cudaStream_t s)
     using namespace hx;
     const bf16* W = n->wh;
     gemm<false, true, kEpiBiasGelu>(B, n->hidden, n->in_dim, n->X, n->in_ld, W + n->oW1, n->in_dim,
-                                    GemmOut{n->w + n->ob1, n->Z1, n->H1, nullptr, n->hidden}, s);
+                                    GemmOut{n->w + n->ob1, n->Z1, n->H1, nullptr, n->hidden}, s, &n->tc);
     gemm<false, true, kEpiBiasGelu>(B, n->hidden, n->hidden, n->H1, n->hidden, W + n->oW2, n->hidden,
-                                    GemmOut{n->w + n->ob2, n->Z2, n->H2, nullptr, n->hidden}, s);
+                                    GemmOut{n->w + n->ob2, n->Z2, n->H2, nullptr, n->hidden}, s, &n->tc);
     gemm<false, true, kEpiBias>(B, n->out_dim, n->hidden, n->H2, n->hidden, W + n->oW3, n->hidden,
-                                GemmOut{n->w + n->ob3, n->Y, nullptr, nullptr, n->out_dim}, s);
+                                GemmOut{n->w + n->ob3, n->Y, nullptr, nullptr, n->out_dim}, s, &n->tc);
 }
 
 // Gradient of every parameter into n->g from dL/dY already in n->dYf / n->dYh.
@@ -531,27 +587,41 @@ void mlp_backward_dy(hx_mlp* n, int B, cudaStream_t s)
     const bf16* W = n->wh;
     // layer 3
     gemm<true, false, kEpiStore>(n->out_dim, n->hidden, B, n->dYh, n->out_dim, n->H2, n->hidden,
-                                 GemmOut{nullptr, n->g + n->oW3, nullptr, nullptr, n->hidden}, s);
+                                 GemmOut{nullptr, n->g + n->oW3, nullptr, nullptr, n->hidden}, s, &n->tc);
     colsum_kernel<<<(n->out_dim + 255) / 256, 256, 0, s>>>(n->dYf, B, n->out_dim, n->out_dim, n->g + n->ob3);
     gemm<false, false, kEpiGeluBack>(B, n->hidden, n->out_dim, n->dYh, n->out_dim, W + n->oW3, n->hidden,
-                                     GemmOut{nullptr, n->dZ2f, n->dZ2h, n->Z2, n->hidden}, s);
+                                     GemmOut{nullptr, n->dZ2f, n->dZ2h, n->Z2, n->hidden}, s, &n->tc);
     // layer 2
     gemm<true, false, kEpiStore>(n->hidden, n->hidden, B, n->dZ2h, n->hidden, n->H1, n->hidden,
-                                 GemmOut{nullptr, n->g + n->oW2, nullptr, nullptr, n->hidden}, s);
+                                 GemmOut{nullptr, n->g + n->oW2, nullptr, nullptr, n->hidden}, s, &n->tc);
     colsum_kernel<<<(n->hidden + 255) / 256, 256, 0, s>>>(n->dZ2f, B, n->hidden, n->hidden, n->g + n->ob2);
     gemm<false, false, kEpiGeluBack>(B, n->hidden, n->hidden, n->dZ2h, n->hidden, W + n->oW2, n->hidden,
-                                     GemmOut{nullptr, n->dZ1f, n->dZ1h, n->Z1, n->hidden}, s);
+                                     GemmOut{nullptr, n->dZ1f, n->dZ1h, n->Z1, n->hidden}, s, &n->tc);
     // layer 1
     gemm<true, false, kEpiStore>(n->hidden, n->in_dim, B, n->dZ1h, n->hidden, n->X, n->in_ld,
-                                 GemmOut{nullptr, n->g + n->oW1, nullptr, nullptr, n->in_dim}, s);
+                                 GemmOut{nullptr, n->g + n->oW1, nullptr, nullptr, n->in_dim}, s, &n->tc);
     colsum_kernel<<<(n->hidden + 255) / 256, 256, 0, s>>>(n->dZ1f, B, n->hidden, n->hidden, n->g + n->ob1);
 }
 
 // Sum of the per-block loss partials (148 blocks) divided by count.
+// Error word of the tensor-core GEMMs (a wait that ran out of its budget); cleared when read.
+int mlp_tc_status(hx_mlp* n, cudaStream_t s)
+{
+    int flag = 0;
+    HX_CUDA_TRY(cudaMemcpyAsync(&flag, n->tc.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HX_CUDA_TRY(cudaStreamSynchronize(s));
+    if (flag != 0) {
+        cudaMemsetAsync(n->tc.err, 0, sizeof(int), s);
+        return fail(HX_ERR_DEVICE_TIMEOUT, "a tensor-core GEMM wait ran out of its iteration budget");
+    }
+    return HX_OK;
+}
+
 int mlp_loss_of_partials(hx_mlp* n, double count, float* loss, cudaStream_t s)
 {
     HX_CUDA_TRY(cudaMemcpyAsync(n->pinned, n->partial, 148 * sizeof(float), cudaMemcpyDeviceToHost, s));
     HX_CUDA_TRY(cudaStreamSynchronize(s));
+    if (int rc = mlp_tc_status(n, s)) return rc;
     double acc = 0.0;
     for (int i = 0; i < 148; ++i) acc += n->pinned[i];
     *loss = static_cast<float>(acc / count);
@@ -582,7 +652,7 @@ void mlp_release(hx_mlp* n)
     if (!n) return;
     if (n->stream) cudaStreamSynchronize(n->stream);
     mlp_free_batch(n);
-    void* p[] = {n->w, n->g, n->m, n->v, n->wh, n->partial};
+    void* p[] = {n->w, n->g, n->m, n->v, n->wh, n->partial, n->tc.err};
     for (void* q : p)
         if (q) cudaFree(q);
     if (n->pinned) cudaFreeHost(n->pinned);
@@ -752,6 +822,8 @@ int hx_mlp_create(uint32_t in_dim, uint32_t hidden, uint32_t out_dim, uint64_t s
     if (e == cudaSuccess) e = cudaMalloc(&n->wh, np * sizeof(bf16));
     if (e == cudaSuccess) e = cudaMalloc(&n->partial, 256 * sizeof(float));
     if (e == cudaSuccess) e = cudaMallocHost(&n->pinned, 256 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&n->tc.err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(n->tc.err, 0, sizeof(int));
     if (e != cudaSuccess) return bail(hx::cuda_fail(e, "cudaMalloc (MLP)"));
     // He-style uniform init from splitmix64(seed), biases zero
     std::vector<float> w(np, 0.f);
@@ -832,7 +904,7 @@ int hx_mlp_forward(hx_mlp* n, const float* x, uint32_t rows, float* y)
     if (e == cudaSuccess) e = cudaStreamSynchronize(n->stream);
     cudaFree(dx);
     if (e != cudaSuccess) return hx::cuda_fail(e, "MLP forward");
-    return HX_OK;
+    return mlp_tc_status(n, n->stream);
 }
 
 int hx_mlp_gradients(hx_mlp* n, const float* x, const float* t, uint32_t rows, float* loss, float* grads,

@@ -1,0 +1,323 @@
+// BF16 GEMM on the 5th-generation tensor cores: C = A B^T with A [M x K] and
+// B [N x K], both row-major (K contiguous), FP32 accumulation in tensor
+// memory, and the closure network's fused epilogues.  Used by the learned
+// closure's MLP (hx_mlp.cu) for its forward and backward GEMMs.  No
+// counterpart in the reference.
+//
+// One CTA of four warps computes a 128 x 128 tile of C:
+//  * warp 0 allocates 128 tensor-memory columns (the 128 x 128 FP32
+//    accumulator, one lane per row) and its lane 0 streams the K blocks of A
+//    and B (128 rows x 64 BF16 each, 16 KB) into a 4-stage shared-memory ring
+//    with TMA tensor loads in the 128-byte swizzled layout;
+//  * lane 0 of warp 1 issues tcgen05.mma (M = 128, N = 128, K = 16, BF16
+//    inputs, FP32 accumulate; four per K block, the shared-memory descriptor
+//    advanced by 32 bytes inside the swizzle atom) and returns each stage to
+//    the producer with tcgen05.commit on that stage's mbarrier;
+//  * after the last block a commit signals the accumulator complete; every
+//    warp then reads its 32 lanes with tcgen05.ld (16 columns at a time) and
+//    applies the epilogue (bias + GELU keeping the pre-activation, bias,
+//    plain store, or GELU backward) straight to global memory.
+// Out-of-range rows, columns and K are zero-filled by the tensor loads and
+// masked at the stores.  Every mbarrier wait is bounded: a wait that runs
+// out sets the error word, the kernel still waits (bounded) for its copies
+// and MMAs in flight, frees its tensor memory and returns.
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+
+#include "hx_internal.h"
+
+namespace hx {
+
+namespace {
+
+constexpr int kBM = 128, kBN = 128, kBK = 64, kStages = 4;
+constexpr uint32_t kTileBytes = kBM * kBK * 2;             // 16 KB, also kBN * kBK * 2
+constexpr uint32_t kStageBytes = 2 * kTileBytes;           // A + B
+constexpr uint32_t kTmemCols = kBN;                        // FP32 accumulator columns
+constexpr uint32_t kSmemBytes = kStages * kStageBytes + 1024 + 256;  // + 1024-byte alignment + barriers
+constexpr uint32_t kPoll = 1u << 22;
+
+// tcgen05.mma instruction descriptor: FP32 accumulator, BF16 A and B, both
+// K-major, N = 128, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kBN >> 3) << 17) | (uint32_t(kBM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Shared-memory matrix descriptor of a K-major tile in the 128-byte swizzled
+// layout: rows of 128 bytes, 8-row atoms 1024 bytes apart (stride byte
+// offset), tile base 1024-byte aligned.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr)
+{
+    uint64_t d = static_cast<uint64_t>((addr & 0x3FFFFu) >> 4);  // start address
+    d |= static_cast<uint64_t>(1) << 16;                         // leading byte offset (unused when swizzled)
+    d |= static_cast<uint64_t>(1024 >> 4) << 32;                 // stride byte offset
+    d |= static_cast<uint64_t>(1) << 46;                         // descriptor version of this architecture
+    d |= static_cast<uint64_t>(2) << 61;                         // 128-byte swizzle
+    return d;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (uint32_t i = 0; i < kPoll; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ float gelu_f(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+
+__device__ __forceinline__ float gelu_grad_f(float z)
+{
+    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+    return cdf + z * pdf;
+}
+
+__global__ void __launch_bounds__(128, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M, int N,
+                   int K, TcGemmOut o, int* err)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const uint32_t raw = saddr(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;  // swizzled tiles need 1024-byte alignment
+    const uint32_t bars = base + kStages * kStageBytes;
+    auto full_bar = [&](int s) { return bars + 8u * s; };
+    auto empty_bar = [&](int s) { return bars + 8u * (kStages + s); };
+    const uint32_t done_bar = bars + 8u * (2 * kStages);
+    const uint32_t tslot = done_bar + 8u;
+    const uint32_t cslot = tslot + 4u;  // K blocks the MMA thread consumed
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+    const int nk = (K + kBK - 1) / kBK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(done_bar, 1);
+        asm volatile("st.shared.u32 [%0], %1;" ::"r"(cslot), "r"(0) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tslot), "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    uint32_t tmem;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(tmem) : "r"(tslot) : "memory");
+
+    int issued = 0;
+    if (warp == 0 && lane == 0) {
+        // ---- producer: TMA loads of the K blocks
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kStages, r = kb / kStages;
+            if (r >= 1 && !mbar_wait(empty_bar(s), (r - 1) & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+            const uint32_t a = base + s * kStageBytes, b = a + kTileBytes;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full_bar(s)), "r"(kStageBytes)
+                         : "memory");
+            tma_load_2d(a, &tmA, kb * kBK, m0, full_bar(s));
+            tma_load_2d(b, &tmB, kb * kBK, n0, full_bar(s));
+            issued = kb + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issue
+        int kb = 0;
+        for (; kb < nk; ++kb) {
+            const int s = kb % kStages, r = kb / kStages;
+            if (!mbar_wait(full_bar(s), r & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+            tc_fence_after();
+            const uint32_t a = base + s * kStageBytes, b = a + kTileBytes;
+#pragma unroll
+            for (int k = 0; k < kBK / 16; ++k) {
+                const uint64_t da = sw128_desc(a + 32u * k), db = sw128_desc(b + 32u * k);
+                const uint32_t accumulate = (kb > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+                    : "memory");
+            }
+            tc_commit(empty_bar(s));  // the stage is free once these MMAs have read it
+        }
+        asm volatile("st.shared.u32 [%0], %1;" ::"r"(cslot), "r"(kb) : "memory");
+        tc_commit(done_bar);  // every MMA issued above has completed
+    }
+
+    // ---- epilogue: every warp reads its 32 accumulator lanes
+    const bool done = mbar_wait(done_bar, 0);
+    if (!done && threadIdx.x == 0) atomicExch(err, 1);
+    tc_fence_after();
+    const int row = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < kBN; c0 += 16) {
+        uint32_t v[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (!done || row >= M) continue;
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+            const int col = n0 + c0 + jj;
+            if (col >= N) break;
+            const float val = __uint_as_float(v[jj]);
+            const long long off = static_cast<long long>(row) * o.ldo + col;
+            if (o.kind == kTcEpiBiasGelu) {
+                const float z = val + o.bias[col];
+                o.outf[off] = z;
+                static_cast<__nv_bfloat16*>(o.outh)[off] = __float2bfloat16(gelu_f(z));
+            } else if (o.kind == kTcEpiBias) {
+                o.outf[off] = val + o.bias[col];
+            } else if (o.kind == kTcEpiStore) {
+                o.outf[off] = val;
+            } else {
+                const float g = val * gelu_grad_f(o.aux[off]);
+                static_cast<__nv_bfloat16*>(o.outh)[off] = __float2bfloat16(g);
+                if (o.outf) o.outf[off] = g;
+            }
+        }
+    }
+
+    // ---- copies still in flight after a wait that ran out land before exit
+    if (warp == 0 && lane == 0) {
+        int consumed;
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(consumed) : "r"(cslot) : "memory");
+        for (int kb = consumed; kb < issued; ++kb) mbar_wait(full_bar(kb % kStages), (kb / kStages) & 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+// Row-major BF16 transpose: out[c][r] = in[r][c] for rows x cols.
+__global__ void transpose_bf16_kernel(const __nv_bfloat16* __restrict__ in, int rows, int cols, int ld_in,
+                                      __nv_bfloat16* __restrict__ out, int ld_out)
+{
+    __shared__ __nv_bfloat16 tile[32][34];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int r = r0 + i, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) tile[i][threadIdx.x] = in[static_cast<long long>(r) * ld_in + c];
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int c = c0 + i, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) out[static_cast<long long>(c) * ld_out + r] = tile[threadIdx.x][i];
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of a row-major BF16 matrix [rows x cols] (leading dimension ld),
+// boxes of 128 rows x 64 columns in the 128-byte swizzled layout.
+bool make_map(CUtensorMap* map, const void* ptr, int rows, int cols, int ld)
+{
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kBK), static_cast<cuuint32_t>(kBM)};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+bool tc_gemm_eligible(const void* A, int lda, const void* B, int ldb)
+{
+    return (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (reinterpret_cast<uintptr_t>(B) % 16 == 0) && lda % 8 == 0 &&
+           ldb % 8 == 0 && encode_fn() != nullptr;
+}
+
+bool tc_gemm(int M, int N, int K, const void* A, int lda, const void* B, int ldb, const TcGemmOut& o, int* err,
+             cudaStream_t s)
+{
+    if (M <= 0 || N <= 0 || K <= 0 || !tc_gemm_eligible(A, lda, B, ldb)) return false;
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return false;
+    if (!configured[dev]) {
+        if (cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kSmemBytes)) != cudaSuccess)
+            return false;
+        configured[dev] = true;
+    }
+    CUtensorMap ma, mb;
+    if (!make_map(&ma, A, M, K, lda) || !make_map(&mb, B, N, K, ldb)) return false;
+    const dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
+    tc_gemm_kernel<<<grid, 128, kSmemBytes, s>>>(ma, mb, M, N, K, o, err);
+    return true;
+}
+
+void launch_transpose_bf16(const void* in, int rows, int cols, int ld_in, void* out, int ld_out, cudaStream_t s)
+{
+    const dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+    transpose_bf16_kernel<<<grid, block, 0, s>>>(static_cast<const __nv_bfloat16*>(in), rows, cols, ld_in,
+                                                 static_cast<__nv_bfloat16*>(out), ld_out);
+}
+
+}  // namespace hx

@@ -50,6 +50,32 @@ def test_mlp_forward_and_gradients_match_oracle():
         off += size
 
 
+@pytest.mark.parametrize("i,h,o,rows", [(64, 256, 64, 300), (40, 512, 24, 1000)])
+def test_mlp_tensor_core_shapes_match_oracle(i, h, o, rows):
+    """Shapes whose GEMMs run on the tensor cores (tcgen05, hx_tcgemm.cu: leading
+    dimensions multiples of 8, hidden >= 128, ragged M and N tiles, K not a
+    multiple of the 64-wide K block): forward and gradients against the FP64
+    restatement with the same BF16 rounding points."""
+    net, p = _net(i, h, o, 11)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((rows, i)).astype(np.float32)
+    t = rng.standard_normal((rows, o)).astype(np.float32)
+    y = net.forward(x)
+    y_ref, loss_ref, g_ref = MO.forward_backward(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64),
+                                                 i, h, o, bf16=True)
+    assert np.max(np.abs(y - y_ref)) <= 1e-4 * max(1.0, np.max(np.abs(y_ref)))
+    loss, g = net.gradients(x, t)
+    assert abs(loss - loss_ref) <= 1e-4 * loss_ref
+    off = 0
+    for name, size in [("W1", h * i), ("b1", h), ("W2", h * h), ("b2", h), ("W3", o * h), ("b3", o)]:
+        gg, rr = g[off:off + size], g_ref[off:off + size]
+        scale = np.max(np.abs(rr))
+        assert np.max(np.abs(gg - rr)) <= 2e-2 * scale, name
+        assert np.corrcoef(gg, rr)[0, 1] > 0.9999, name
+        off += size
+    net.close()
+
+
 def test_mlp_training_reduces_loss():
     i, h, o = 32, 64, 16
     rng = np.random.default_rng(2)
