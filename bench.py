@@ -269,7 +269,8 @@ def reference_cuda(cfg: dict, p, steps: int) -> dict:
         try:
             r = subprocess.run([binary, "--time", str(k), "--warmup", "1"], env=env, capture_output=True,
                                text=True, timeout=900)
-            line = json.loads(r.stdout.strip().splitlines()[-1])
+            # the reference prints its own diagnostics on stdout too; the driver's line is the last JSON object
+            line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
         except (subprocess.SubprocessError, ValueError, IndexError) as e:
             out[name] = {"unavailable": f"run failed: {type(e).__name__}"}
             continue
@@ -477,12 +478,14 @@ def run_ours(args, cfg: dict) -> None:
     achieved = per_launch_bytes / (launch_ms / 1000.0) / 1e9
     peak, peak_kind = load_peaks()
     packed = bool(ctx.hermitian_packed)
-    kernel = "herm_kernel" if packed else "fused_kernel"
+    kernel = "small_kernel" if ctx.stage_path == "small" else ("herm_kernel" if packed else "fused_kernel")
     # DRAM bytes of one stage: the stage kernel plus the up-term kernel (committed ncu summaries)
     traffic = profiled_traffic(args.config, kernel)
+    traffic_files = [f"profiles/{kernel}_{args.config}_ncu.txt"]
     up_traffic = profiled_traffic(args.config, "upterm_kernel")
     if traffic is not None and up_traffic is not None and info_kernels_per_stage(ctx) == 2:
         traffic += up_traffic
+        traffic_files.append(f"profiles/upterm_kernel_{args.config}_ncu.txt")
     slab_elems = p.dim * (p.dim + 1) // 2 if packed else p.dim * p.dim
 
     # ---- end to end through the C ABI with host buffers (e2e) --------------
@@ -537,9 +540,8 @@ def run_ours(args, cfg: dict) -> None:
                          else "fallback 6650 GB/s",
                          "algorithmic_bytes_per_launch": per_launch_bytes,
                          "kernel": stage_kernels_label(ctx, p, packed, info_kernels_per_stage(ctx)),
-                         "traffic_source": (f"dram bytes of one stage from profiles/{kernel}_{args.config}_ncu.txt "
-                                            f"+ profiles/upterm_kernel_{args.config}_ncu.txt") if traffic is not None
-                         else "no ncu summary of this workload under profiles/",
+                         "traffic_source": ("dram bytes of one stage from " + " + ".join(traffic_files))
+                         if traffic is not None else "no ncu summary of this workload under profiles/",
                          "launch_ms": launch_ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": slab_elems * 16 + 24,

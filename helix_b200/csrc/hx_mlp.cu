@@ -167,7 +167,7 @@ bool tc_enabled()
 {
     static const bool v = [] {
         const char* e = std::getenv("HX_TC_GEMM");
-        return e && e[0] == '1';
+        return !(e && e[0] == '0');
     }();
     return v;
 }
