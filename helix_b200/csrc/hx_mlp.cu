@@ -205,14 +205,28 @@ void gemm(int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb, c
     gemm_kernel<TA, TB, EPI><<<grid, GT, 0, s>>>(M, N, K, A, lda, B, ldb, o);
 }
 
-// column sums of an FP32 matrix [rows x cols] (bias gradients); fixed order
+// column sums of an FP32 matrix [rows x cols] (bias gradients) in a fixed
+// order: block (32, 8) per 32 columns, thread (tx, ty) sums rows ty, ty + 8,
+// ... of column tx (coalesced), then the 8 partial sums are added in order
 __global__ void colsum_kernel(const float* __restrict__ x, int rows, int cols, int ld, float* out)
 {
-    const int cidx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cidx >= cols) return;
+    __shared__ float part[8][33];
+    const int c = blockIdx.x * 32 + threadIdx.x;
     float s = 0.f;
-    for (int r = 0; r < rows; ++r) s += x[static_cast<long long>(r) * ld + cidx];
-    out[cidx] = s;
+    if (c < cols)
+        for (int r = threadIdx.y; r < rows; r += 8) s += x[static_cast<long long>(r) * ld + c];
+    part[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0 && c < cols) {
+        float t = 0.f;
+        for (int k = 0; k < 8; ++k) t += part[k][threadIdx.x];
+        out[c] = t;
+    }
+}
+
+void colsum(const float* x, int rows, int cols, int ld, float* out, cudaStream_t s)
+{
+    colsum_kernel<<<(cols + 31) / 32, dim3(32, 8), 0, s>>>(x, rows, cols, ld, out);
 }
 
 // residual R = Y - T, dY = 2 R / (rows cols) (FP32 and BF16); per-block partial sums of R^2
@@ -588,19 +602,19 @@ void mlp_backward_dy(hx_mlp* n, int B, cudaStream_t s)
     // layer 3
     gemm<true, false, kEpiStore>(n->out_dim, n->hidden, B, n->dYh, n->out_dim, n->H2, n->hidden,
                                  GemmOut{nullptr, n->g + n->oW3, nullptr, nullptr, n->hidden}, s, &n->tc);
-    colsum_kernel<<<(n->out_dim + 255) / 256, 256, 0, s>>>(n->dYf, B, n->out_dim, n->out_dim, n->g + n->ob3);
+    colsum(n->dYf, B, n->out_dim, n->out_dim, n->g + n->ob3, s);
     gemm<false, false, kEpiGeluBack>(B, n->hidden, n->out_dim, n->dYh, n->out_dim, W + n->oW3, n->hidden,
                                      GemmOut{nullptr, n->dZ2f, n->dZ2h, n->Z2, n->hidden}, s, &n->tc);
     // layer 2
     gemm<true, false, kEpiStore>(n->hidden, n->hidden, B, n->dZ2h, n->hidden, n->H1, n->hidden,
                                  GemmOut{nullptr, n->g + n->oW2, nullptr, nullptr, n->hidden}, s, &n->tc);
-    colsum_kernel<<<(n->hidden + 255) / 256, 256, 0, s>>>(n->dZ2f, B, n->hidden, n->hidden, n->g + n->ob2);
+    colsum(n->dZ2f, B, n->hidden, n->hidden, n->g + n->ob2, s);
     gemm<false, false, kEpiGeluBack>(B, n->hidden, n->hidden, n->dZ2h, n->hidden, W + n->oW2, n->hidden,
                                      GemmOut{nullptr, n->dZ1f, n->dZ1h, n->Z1, n->hidden}, s, &n->tc);
     // layer 1
     gemm<true, false, kEpiStore>(n->hidden, n->in_dim, B, n->dZ1h, n->hidden, n->X, n->in_ld,
                                  GemmOut{nullptr, n->g + n->oW1, nullptr, nullptr, n->in_dim}, s, &n->tc);
-    colsum_kernel<<<(n->hidden + 255) / 256, 256, 0, s>>>(n->dZ1f, B, n->hidden, n->hidden, n->g + n->ob1);
+    colsum(n->dZ1f, B, n->hidden, n->hidden, n->g + n->ob1, s);
 }
 
 // Sum of the per-block loss partials (148 blocks) divided by count.
