@@ -26,6 +26,7 @@ STATUS_NAMES = {
 PRECISION_DOUBLE = 1
 PRECISION_MIXED = 2  # complex64 hierarchy, ADO 0 (rho_0) in double precision
 FLAG_FULL_STATE = 1  # keep full d x d slabs on the device (contexts with 32 <= d <= 1024 default to Hermitian-packed)
+FLAG_DENSE_H = 2  # Hamiltonian commutator as tensor-core products (mixed precision, full slabs, 128 <= d <= 1024)
 
 # Every exported symbol of include/helix_b200.h
 EXPORTS = [
@@ -88,7 +89,7 @@ class Info(C.Structure):
 
 
 # hx_info.stage_path (HX_PATH_*)
-STAGE_PATHS = {0: "generic", 1: "fused", 2: "band", 3: "flip", 4: "csr", 5: "small"}
+STAGE_PATHS = {0: "generic", 1: "fused", 2: "band", 3: "flip", 4: "csr", 5: "small", 6: "dense"}
 
 
 class Counters(C.Structure):
@@ -309,15 +310,18 @@ class Context:
 
     For 32 <= d <= 1024 the device keeps Hermitian-packed slabs and
     ``set_state`` accepts Hermitian ADOs only; ``full_state=True`` keeps full slabs for
-    general states (HX_FLAG_FULL_STATE)."""
+    general states (HX_FLAG_FULL_STATE).  ``dense_h=True`` (with ``precision="mixed"``)
+    applies H as a dense matrix on the tensor cores (HX_FLAG_DENSE_H; full slabs,
+    Hermitian states)."""
 
     def __init__(self, problem, order: int = 4, dt: float | None = None, precision: str = "double",
-                 full_state: bool = False):
+                 full_state: bool = False, dense_h: bool = False):
         L = lib()
         self.problem = problem
         d = problem.dim
         prec = {"double": PRECISION_DOUBLE, "mixed": PRECISION_MIXED}[precision]
-        prob, self._keep = _problem_struct(problem, order, dt, prec, FLAG_FULL_STATE if full_state else 0)
+        flags = (FLAG_FULL_STATE if full_state or dense_h else 0) | (FLAG_DENSE_H if dense_h else 0)
+        prob, self._keep = _problem_struct(problem, order, dt, prec, flags)
         h = C.c_void_p()
         _check(L.hx_ctx_create(C.byref(prob), C.byref(h)))
         self._h = h
@@ -326,7 +330,7 @@ class Context:
         self.dim = d
         # device slabs hold the upper triangle only (see herm_index)
         self.hermitian_packed = (d >= 32 and int(self.info.state_bytes) == self.size * (d * (d + 1) // 2) * 16)
-        # stage kernels in use: "fused", "band", "flip", "csr" or "generic"
+        # stage kernels in use: one of the names in STAGE_PATHS
         self.stage_path = STAGE_PATHS[int(self.info.stage_path)]
 
     # lifecycle -----------------------------------------------------------

@@ -57,7 +57,8 @@ void release(hx_ctx* c)
                     c->ent_wc, c->ent_wa, c->order_perm, c->ado_keep, c->up_slot, c->up_ado, c->up_cnt,
                     c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf, c->rho32, c->ua32, c->ub32,
                     c->U32, c->diag32, c->vdiag32, c->hflip32, c->diag_herm, c->vbit, c->csr_ptr, c->csr_col,
-                    c->csr_val, c->pack_scale, c->pack_bad};
+                    c->csr_val, c->pack_scale, c->pack_bad, c->dense_hr, c->dense_hr_lo, c->dense_xhi,
+                    c->dense_xlo, c->dense_y, c->dense_h64};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -207,6 +208,7 @@ hx::LargeArgs<float> large_args32(const hx_ctx* c)
     a.logd = c->logd;
     a.first_ado = 1;
     a.herm = c->herm ? 1 : 0;
+    a.dense_y = c->dense ? c->dense_y : nullptr;
     return a;
 }
 
@@ -219,15 +221,38 @@ hx::LargeUpArgs<R> large_up_args(const hx_ctx* c, const R* vdiag)
 hx::Ado0Args ado0_args(const hx_ctx* c)
 {
     return hx::Ado0Args{c->herm ? c->diag_herm : c->diag_table, c->vdiag, c->hflip, c->ent_count, c->ent_slab, c->ent_bath,
-                        c->ent_wc, c->ent_wa, c->M, c->J, c->logd, c->herm ? 1 : 0};
+                        c->ent_wc, c->ent_wa, c->M, c->J, c->logd, c->herm ? 1 : 0,
+                        c->dense ? c->dense_y : nullptr, c->dense ? c->dense_h64 : nullptr};
 }
 
 // Index of a state buffer of the context: 0 = rho, 1 = ua, 2 = ub.
 int buffer_id(const hx_ctx* c, const double2* p) { return p == c->rho ? 0 : (p == c->ua ? 1 : 2); }
 
+// Dense H: Y_n = X_n H_off (H without its diagonal, which the band kernels
+// apply exactly) for every ADO of the complex64 stage input u32, as the real
+// product [H d x 2d] x [2d x 2d] (interleaved complex rows of X times the
+// real form of H_off) in 3-term TF32 split form, X_hi H_hi + X_hi H_lo +
+// X_lo H_hi, FP32 accumulation.  Returns kernels launched.
+int launch_dense_product(hx_ctx* c, const float2* u32)
+{
+    const long long n = 2ll * c->H * static_cast<long long>(c->slab);
+    hx::launch_tf32_split(reinterpret_cast<const float*>(u32), c->dense_xhi, c->dense_xlo, n, c->stream);
+    const int d2 = 2 * c->d;
+    const float *xh = c->dense_xhi, *xl = c->dense_xlo;
+    const hx::TcPair pairs[3] = {{xh, d2, c->dense_hr, d2}, {xh, d2, c->dense_hr_lo, d2}, {xl, d2, c->dense_hr, d2}};
+    hx::TcGemmOut o{};
+    o.kind = hx::kTcEpiStore;
+    o.outf = reinterpret_cast<float*>(c->dense_y);
+    o.ldo = d2;
+    if (!hx::tc_gemm_sum(static_cast<int>(c->H * c->d), d2, d2, 3, pairs, true, o, c->error_flag, c->stream))
+        c->launch_failed = true;
+    return 2;
+}
+
 // One stage of the band kernels (hx_large.cu): the up-term kernel of tier
 // L-1, the band kernel over the hierarchy and, in mixed precision, the
-// double-precision kernel of ADO 0.  Returns kernels launched.
+// double-precision kernel of ADO 0 (with a dense H, the tensor-core product
+// first).  Returns kernels launched.
 int launch_large_stage(hx_ctx* c, const double2* u, const double2* rho, double2* out, double alpha, int base)
 {
     int k = 0;
@@ -242,6 +267,7 @@ int launch_large_stage(hx_ctx* c, const double2* u, const double2* rho, double2*
     float2* b32[3] = {c->rho32, c->ua32, c->ub32};
     const float2* u32 = b32[buffer_id(c, u)];
     float2* o32 = b32[buffer_id(c, out)];
+    if (c->dense) k += launch_dense_product(c, u32);
     if (c->up_slots > 0) {
         hx::launch_large_upterm<float>(large_up_args<float>(c, c->vdiag32), u32, c->U32, c->stream);
         ++k;
@@ -324,7 +350,8 @@ int enqueue_step(hx_ctx* c)
 // Energy and trace of rho_0 into out[0..2].
 void launch_obs(hx_ctx* c, double* out)
 {
-    if (c->use_csr) hx::launch_observables_csr(c->rho, c->logd, c->csr_ptr, c->csr_col, c->csr_val, out, c->stream);
+    if (c->use_csr || c->dense)
+        hx::launch_observables_csr(c->rho, c->logd, c->csr_ptr, c->csr_col, c->csr_val, out, c->stream);
     else hx::launch_observables(c->rho, c->logd, c->herm, c->hdiag, c->hflip, nullptr, out, c->stream);
 }
 
@@ -337,6 +364,10 @@ int check_launch(const char* what)
 
 int read_error_flag(hx_ctx* c)
 {
+    if (c->launch_failed) {
+        c->launch_failed = false;
+        return fail(HX_ERR_UNSUPPORTED_EXECUTION, "the tensor-core product of a stage could not be enqueued");
+    }
     int flag = 0;
     HX_CUDA_TRY(cudaMemcpyAsync(&flag, c->error_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -369,6 +400,17 @@ bool pack_herm_host(const double* in, int logd, double2* pk, double rel_tol = 1e
                         : make_double2(in[2 * up], in[2 * up + 1]);
     }
     return true;
+}
+
+// FP32 value rounded to TF32 (10 mantissa bits, to nearest, ties away from
+// zero): the host twin of the device-side split in hx_tcgemm.cu.
+float tf32_round_host(float v)
+{
+    uint32_t u;
+    std::memcpy(&u, &v, sizeof(u));
+    u = (u + 0x1000u) & 0xFFFFE000u;
+    std::memcpy(&v, &u, sizeof(u));
+    return v;
 }
 
 // f(k) for k in [0, n) on up to 16 host threads.
@@ -632,9 +674,39 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     if (p->n_baths == 0 || !p->baths) return fail(HX_ERR_UNSUPPORTED_BATH, "at least one bath is required");
     if (p->n_baths > static_cast<uint32_t>(hx::kMaxBaths)) return fail(HX_ERR_UNSUPPORTED_BATH, "too many baths");
     if (p->max_depth < 1) return fail(HX_ERR_UNSUPPORTED_HIERARCHY, "max_depth must be >= 1");
-    if ((p->flags & ~HX_FLAG_FULL_STATE) != 0) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "unknown flags");
+    if ((p->flags & ~(HX_FLAG_FULL_STATE | HX_FLAG_DENSE_H)) != 0)
+        return fail(HX_ERR_INVALID_RUNTIME_OPTION, "unknown flags");
 
     const int J = static_cast<int>(p->n_baths);
+    // dense H on the tensor cores: the band kernels see only the diagonal of
+    // H, the rest is applied as matrix products before every stage
+    const bool want_dense = (p->flags & HX_FLAG_DENSE_H) != 0;
+    HostCsr dense_h;
+    hx_problem dense_problem;
+    std::vector<double> dense_diag, dense_zero;
+    if (want_dense) {
+        if (p->precision != HX_PRECISION_MIXED || !(p->flags & HX_FLAG_FULL_STATE))
+            return fail(HX_ERR_UNSUPPORTED_EXECUTION, "HX_FLAG_DENSE_H needs HX_PRECISION_MIXED and HX_FLAG_FULL_STATE");
+        std::string why;
+        if (p->h_csr) {
+            if (!take_csr(p->h_csr, static_cast<int>(d), dense_h, why, "h_csr"))
+                return fail(HX_ERR_INVALID_RUNTIME_OPTION, why);
+        } else {
+            dense_h = flip_csr(p->h_diag, p->h_flip, static_cast<int>(d), logd);
+        }
+        // the real diagonal of H stays exact in the band kernels' diagonal table; the
+        // products carry only the off-diagonal part (smaller terms, smaller rounding)
+        dense_diag.assign(d, 0.0);
+        for (uint32_t r = 0; r < d; ++r)
+            for (int q = dense_h.ptr[r]; q < dense_h.ptr[r + 1]; ++q)
+                if (dense_h.col[q] == static_cast<int32_t>(r)) dense_diag[r] += dense_h.val[q].x;
+        dense_zero.assign(d, 0.0);
+        dense_problem = *p;
+        dense_problem.h_csr = nullptr;
+        dense_problem.h_diag = dense_diag.data();
+        dense_problem.h_flip = dense_zero.data();
+        p = &dense_problem;
+    }
     // general sparse operators: checked and gathered here, run on the CSR path
     // unless every operator is a diagonal plus single-spin flips (then the
     // problem is rewritten in that form and takes the faster paths)
@@ -744,6 +816,19 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
     c->mixed = p->precision == HX_PRECISION_MIXED;
     if (c->mixed && !c->use_large)
         return bail(fail(HX_ERR_UNSUPPORTED_PRECISION, "mixed precision needs diagonal coupling operators"));
+    if (want_dense) {
+        if (!c->use_large)
+            return bail(fail(HX_ERR_UNSUPPORTED_EXECUTION,
+                             "HX_FLAG_DENSE_H needs 128 <= d <= 1024 and diagonal coupling operators"));
+        if (static_cast<long long>(H) * d > INT32_MAX)
+            return bail(fail(HX_ERR_UNSUPPORTED_EXECUTION, "HX_FLAG_DENSE_H: H d exceeds the GEMM's row range"));
+        if (!hx::tc_gemm_ready(true))
+            return bail(fail(HX_ERR_UNSUPPORTED_EXECUTION, "HX_FLAG_DENSE_H: the tensor-core GEMM is unavailable"));
+        for (const double2& v : dense_h.val)
+            if (!std::isfinite(v.x) || !std::isfinite(v.y))
+                return bail(fail(HX_ERR_INVALID_RUNTIME_OPTION, "H is not finite"));
+        c->dense = true;
+    }
     // fused stage kernels (d = 32, 64), on Hermitian-packed slabs unless the caller keeps full slabs
     const char* force_generic = std::getenv("HX_FORCE_GENERIC_STAGE");
     const bool want_herm = (p->flags & HX_FLAG_FULL_STATE) == 0;
@@ -831,6 +916,45 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
         (rc = upload(c, c->vdiag, vd)) || (rc = upload(c, c->xi, xi)) || (rc = upload(c, c->counter, ct)) ||
         (rc = upload(c, c->bath_off, off)))
         return bail(rc);
+    if (c->dense) {
+        // the real form of H without its diagonal (TF32 split) for Y = X H, stage scratch,
+        // and the whole H in CSR for the energy
+        const size_t D = d, W = 2 * D;
+        std::vector<double> hre(D * D, 0.0), him(D * D, 0.0);
+        for (size_t r = 0; r < D; ++r)
+            for (int q = dense_h.ptr[r]; q < dense_h.ptr[r + 1]; ++q)
+                if (dense_h.col[q] != static_cast<int32_t>(r)) {
+                    hre[r * D + dense_h.col[q]] += dense_h.val[q].x;
+                    him[r * D + dense_h.col[q]] += dense_h.val[q].y;
+                }
+        std::vector<double2> h64(D * D);
+        for (size_t i = 0; i < D * D; ++i) h64[i] = make_double2(hre[i], him[i]);
+        std::vector<float> hi(W * W), lo(W * W);
+        auto put = [&](size_t row, size_t k, double v) {
+            const float h = tf32_round_host(static_cast<float>(v));
+            hi[row * W + k] = h;
+            lo[row * W + k] = tf32_round_host(static_cast<float>(v - static_cast<double>(h)));
+        };
+        for (size_t cc = 0; cc < D; ++cc)
+            for (size_t k = 0; k < D; ++k) {
+                const double re = hre[k * D + cc], im = him[k * D + cc];
+                put(2 * cc, 2 * k, re);
+                put(2 * cc, 2 * k + 1, -im);
+                put(2 * cc + 1, 2 * k, im);
+                put(2 * cc + 1, 2 * k + 1, re);
+            }
+        if ((rc = dev_alloc(c, &c->dense_h64, h64.size())) || (rc = upload(c, c->dense_h64, h64)) ||
+            (rc = dev_alloc(c, &c->dense_hr, hi.size())) || (rc = dev_alloc(c, &c->dense_hr_lo, lo.size())) ||
+            (rc = upload(c, c->dense_hr, hi)) || (rc = upload(c, c->dense_hr_lo, lo)) ||
+            (rc = dev_alloc(c, &c->dense_xhi, 2 * nstate)) || (rc = dev_alloc(c, &c->dense_xlo, 2 * nstate)) ||
+            (rc = dev_alloc(c, &c->dense_y, nstate)) || (rc = dev_alloc(c, &c->csr_ptr, dense_h.ptr.size())) ||
+            (rc = dev_alloc(c, &c->csr_col, std::max<size_t>(1, dense_h.col.size()))) ||
+            (rc = dev_alloc(c, &c->csr_val, std::max<size_t>(1, dense_h.val.size()))) ||
+            (rc = upload(c, c->csr_ptr, dense_h.ptr)))
+            return bail(rc);
+        if (!dense_h.col.empty() && ((rc = upload(c, c->csr_col, dense_h.col)) || (rc = upload(c, c->csr_val, dense_h.val))))
+            return bail(rc);
+    }
 
     // per-mode temporaries for the coefficient kernel
     int32_t *dmb = nullptr, *dmk = nullptr;
@@ -991,9 +1115,10 @@ int hx_ctx_info(const hx_ctx* c, hx_info* info)
     info->steps_done = c->steps_done;
     info->time = static_cast<double>(c->steps_done) * c->dt;
     int per_stage = (c->use_flip || c->use_csr || (c->use_fused && c->up_slots > 0)) ? 2 : 1;
-    if (c->use_large) per_stage = 1 + (c->up_slots > 0 ? 1 : 0) + (c->mixed ? 1 : 0);
+    if (c->use_large) per_stage = 1 + (c->up_slots > 0 ? 1 : 0) + (c->mixed ? 1 : 0) + (c->dense ? 2 : 0);
     info->kernels_per_step = static_cast<uint32_t>(c->order) * per_stage;
-    info->stage_path = c->use_csr ? HX_PATH_CSR
+    info->stage_path = c->dense     ? HX_PATH_DENSE
+                       : c->use_csr ? HX_PATH_CSR
                        : c->use_flip ? HX_PATH_FLIP
                        : c->use_large ? HX_PATH_BAND
                        : c->use_fused ? HX_PATH_FUSED
@@ -1158,6 +1283,26 @@ int hx_ctx_write_state(hx_ctx* c, const double* in, uint64_t n)
         c->counters.h2d_bytes += tmp.size() * sizeof(float2) + P * sizeof(double2);
         HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
         return HX_OK;
+    }
+    if (c->dense) {
+        // the tensor-core product takes H X_n as (X_n H)^dagger, which needs Hermitian ADOs
+        std::vector<char> ok(static_cast<size_t>(c->H), 1);
+        parallel_for(c->H, [&](long long k) {
+            const double* x = in + 2 * static_cast<size_t>(k) * c->slab;
+            double scale2 = 0.0, worst2 = 0.0;
+            for (int r = 0; r < c->d; ++r)
+                for (int cc = 0; cc < c->d; ++cc) {
+                    const size_t up = static_cast<size_t>(r) * c->d + cc, lo = static_cast<size_t>(cc) * c->d + r;
+                    scale2 = std::max(scale2, x[2 * up] * x[2 * up] + x[2 * up + 1] * x[2 * up + 1]);
+                    const double dr = x[2 * up] - x[2 * lo], di = x[2 * up + 1] + x[2 * lo + 1];
+                    worst2 = std::max(worst2, dr * dr + di * di);
+                }
+            ok[k] = !(worst2 > 1e-24 * scale2);
+        });
+        for (long long k = 0; k < c->H; ++k)
+            if (!ok[k])
+                return fail(HX_ERR_INVALID_RUNTIME_OPTION,
+                            "ADO " + std::to_string(k) + " is not Hermitian, which HX_FLAG_DENSE_H requires");
     }
     if (c->mixed) {
         std::vector<float2> tmp(count);

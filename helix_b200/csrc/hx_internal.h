@@ -167,6 +167,20 @@ struct TcGemmOut {
 bool tc_gemm_eligible(const void* A, int lda, const void* B, int ldb);
 bool tc_gemm(int M, int N, int K, const void* A, int lda, const void* B, int ldb, const TcGemmOut& o, int* err,
              cudaStream_t s);
+// Sum of up to three products A_p B_p^T in one accumulator, BF16 or FP32 operands (the latter on the TF32
+// path): the terms of a split-precision product.  Leading dimensions multiples of 16 bytes.
+struct TcPair {
+    const void* A;
+    int lda;
+    const void* B;
+    int ldb;
+};
+bool tc_gemm_sum(int M, int N, int K, int npairs, const TcPair* pairs, bool tf32, const TcGemmOut& o, int* err,
+                 cudaStream_t s);
+// The driver entry point and kernel attributes the tensor-core GEMM needs are available.
+bool tc_gemm_ready(bool tf32);
+// TF32 split of n floats (16-byte aligned): hi = tf32(x), lo = tf32(x - hi), both exact TF32 values
+void launch_tf32_split(const float* x, float* hi, float* lo, long long n, cudaStream_t s);
 void launch_transpose_bf16(const void* in, int rows, int cols, int ld_in, void* out, int ld_out, cudaStream_t s);
 // d <= 16, full slabs, sigma_z couplings, every up term in the entry lists: batched gathers (hx_small.cu)
 size_t small_smem(int logd, int M);
@@ -223,6 +237,10 @@ struct LargeArgs {
     int M, J, logd;
     int first_ado;           // 1 when ADO 0 runs in double precision (ado0_kernel)
     int herm;                // 1: slabs, diag and U Hermitian-packed (herm_band_kernel)
+    // dense H on the tensor cores (HX_FLAG_DENSE_H, full slabs): Y_n = X_n H_off for every ADO (H_off: H
+    // without its diagonal), in the state layout; X_n is Hermitian, so H_off X_n = Y_n^dagger and
+    // -i[H_off, X_n]_rc = -i(conj(Y_cr) - Y_rc)
+    const C2<R>* dense_y;
 };
 template <typename R>
 struct LargeUpArgs {
@@ -243,6 +261,8 @@ struct Ado0Args {
     const double* ent_wa;
     int M, J, logd;
     int herm;                // 1: the slabs (and diag) are Hermitian-packed
+    const float2* dense_y;   // dense H: Y_0 = X_0 H_off (as in LargeArgs), else nullptr
+    const double2* dense_h;  // dense H: H_off [d][d] in FP64 (the diagonal of the commutator, exactly traceless)
 };
 bool large_supported(int logd, int M, int J);
 template <typename R> bool prepare_large(const LargeArgs<R>& a);  // shared-memory limit; call before capture
@@ -405,6 +425,15 @@ struct hx_ctx {
     double2* state_pinned = nullptr; // pinned staging for packed whole-state transfers
     double* pack_scale = nullptr;    // [H] per-slab scale of the device-side packer (first use)
     int* pack_bad = nullptr;         // first ADO that failed the packer's Hermiticity check
+    // dense H (HX_FLAG_DENSE_H): Y = X H on the tensor cores before every stage
+    bool dense = false;
+    float* dense_hr = nullptr;    // [2d][2d] real form of H_off, K-major: row 2c = (Re H_kc, -Im H_kc)_k,
+    float* dense_hr_lo = nullptr; //   row 2c+1 = (Im H_kc, Re H_kc)_k; and its TF32 residual
+    float* dense_xhi = nullptr;   // [H][d][2d] TF32 split of the stage input
+    float* dense_xlo = nullptr;
+    float2* dense_y = nullptr;    // [H][d][d] Y_n = X_n H_off (H without its diagonal)
+    double2* dense_h64 = nullptr; // [d][d] H_off in FP64 (ADO 0's diagonal commutator terms)
+    bool launch_failed = false;   // a stage could not be enqueued (reported by the next error check)
     size_t state_pinned_elems = 0;
     size_t device_bytes = 0;
     hx_counters counters{};

@@ -17,6 +17,14 @@
 //    entries at a time; the up term of tier L-1 (neighbours in the top tier)
 //    comes from large_upterm_kernel, which walks the top tier tile by tile.
 //
+// With a dense H (HX_FLAG_DENSE_H, complex64 path) the diagonal table keeps
+// the real diagonal of H and the commutator with the rest of H (no flip
+// terms) comes from the product Y_n = X_n H_off of every ADO, computed before
+// the stage by the tensor-core GEMM (hx_tcgemm.cu) as one [H d x 2d] x
+// [2d x 2d] real product in 3-term TF32 split form.  Every ADO is Hermitian,
+// so H_off X_n = Y_n^dagger and -i[H_off, X_n]_rc = -i(conj(Y_cr) - Y_rc): one
+// product per ADO, not two.
+//
 // The reference has no precision other than the compiled one
 // (src/legacy_compile_options.h:6); the complex64 path is the
 // mixed-precision extension of this propagator.
@@ -139,6 +147,14 @@ __global__ void __launch_bounds__(256, 2)
             const R tr = t[kk].x - g;
             acc[k0 + kk].x = tr * x[kk].x - t[kk].y * x[kk].y + hi;
             acc[k0 + kk].y = tr * x[kk].y + t[kk].y * x[kk].x - hr;
+            if (a.dense_y) {
+                // -i [H_off, X] = -i (conj(Y_cr) - Y_rc) from the tensor-core product Y = X H_off
+                const int r = static_cast<int>(ge >> LOGD), c = static_cast<int>(ge & (D - 1));
+                const C* yn = a.dense_y + n * D2;
+                const C yrc = __ldg(yn + ge), ycr = __ldg(yn + (static_cast<long long>(c) << LOGD) + r);
+                acc[k0 + kk].x -= yrc.y + ycr.y;
+                acc[k0 + kk].y += yrc.x - ycr.x;
+            }
         }
     }
     // ---- neighbour entries, two at a time, CH elements per load batch
@@ -473,6 +489,24 @@ __global__ void __launch_bounds__(256)
     }
     double ax = t.x * x.x - t.y * x.y + hi;
     double ay = t.x * x.y + t.y * x.x - hr;
+    if (a.dense_y && r != c) {
+        // -i [H_off, X] = -i (conj(Y_cr) - Y_rc) of ADO 0 from the tensor-core product Y = X H_off
+        const float2 yrc = a.dense_y[ge], ycr = a.dense_y[(static_cast<long long>(c) << a.logd) + r];
+        ax -= static_cast<double>(yrc.y) + static_cast<double>(ycr.y);
+        ay += static_cast<double>(yrc.x) - static_cast<double>(ycr.x);
+    } else if (a.dense_y) {
+        // diagonal: -i [H_off, X]_rr = -2 Im z_r, z_r = sum_k X_rk conj(H_rk) (X, H Hermitian), in FP64 so
+        // that the commutator stays traceless (sum_r Im z_r = Im Tr(X H) = 0) to FP64 rounding
+        const double2* xr = u0 + (static_cast<long long>(r) << a.logd);
+        const double2* hr_row = a.dense_h + (static_cast<long long>(r) << a.logd);
+        double z0 = 0.0, z1 = 0.0;
+        for (int k = 0; k < D; k += 2) {
+            const double2 x0 = xr[k], h0 = hr_row[k], x1 = xr[k + 1], h1 = hr_row[k + 1];
+            z0 += x0.y * h0.x - x0.x * h0.y;
+            z1 += x1.y * h1.x - x1.x * h1.y;
+        }
+        ax -= 2.0 * (z0 + z1);
+    }
     const int Q = a.ent_count[0];
     for (int q = 0; q < Q; ++q) {
         const int j = a.ent_bath[q] & 0xffff;

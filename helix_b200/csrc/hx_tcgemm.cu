@@ -1,22 +1,28 @@
-// BF16 GEMM on the 5th-generation tensor cores: C = A B^T with A [M x K] and
-// B [N x K], both row-major (K contiguous), FP32 accumulation in tensor
-// memory, and the closure network's fused epilogues.  Used by the learned
-// closure's MLP (hx_mlp.cu) for its forward and backward GEMMs.  No
-// counterpart in the reference.
+// GEMM on the 5th-generation tensor cores: C = sum_p A_p B_p^T (one to three
+// operand pairs in one accumulator) with A_p [M x K] and B_p [N x K], both
+// row-major (K contiguous), BF16 (kind::f16) or TF32 (kind::tf32) operands and
+// FP32 accumulation in tensor memory.  Used by the learned closure's MLP
+// (hx_mlp.cu; BF16, one pair, fused bias / GELU epilogues) and by the dense-H
+// stage (hx_ctx.cu; TF32, the three pairs of a split product, plain store).
+// No counterpart in the reference.
 //
-// One CTA of four warps computes a 128 x 128 tile of C:
+// One CTA of four warps computes a 128 x 128 tile of C (1-D grid, N tiles
+// fastest):
 //  * warp 0 allocates 128 tensor-memory columns (the 128 x 128 FP32
-//    accumulator, one lane per row) and its lane 0 streams the K blocks of A
-//    and B (128 rows x 64 BF16 each, 16 KB) into a 4-stage shared-memory ring
-//    with TMA tensor loads in the 128-byte swizzled layout;
-//  * lane 0 of warp 1 issues tcgen05.mma (M = 128, N = 128, K = 16, BF16
-//    inputs, FP32 accumulate; four per K block, the shared-memory descriptor
-//    advanced by 32 bytes inside the swizzle atom) and returns each stage to
-//    the producer with tcgen05.commit on that stage's mbarrier;
+//    accumulator, one lane per row) and its lane 0 streams the K blocks of
+//    every pair (128 rows x 128 bytes of A and of B: 64 BF16 or 32 TF32, 16 KB
+//    each) into a 4-stage shared-memory ring with TMA tensor loads in the
+//    128-byte swizzled layout;
+//  * lane 0 of warp 1 issues tcgen05.mma (M = 128, N = 128, 32 bytes of K per
+//    instruction: K = 16 BF16 or 8 TF32; four per K block, the shared-memory
+//    descriptor advanced by 32 bytes inside the swizzle atom) and returns each
+//    stage to the producer with tcgen05.commit on that stage's mbarrier;
 //  * after the last block a commit signals the accumulator complete; every
-//    warp then reads its 32 lanes with tcgen05.ld (16 columns at a time) and
-//    applies the epilogue (bias + GELU keeping the pre-activation, bias,
-//    plain store, or GELU backward) straight to global memory.
+//    warp reads its 32 lanes with tcgen05.ld (16 columns at a time) into a
+//    padded shared-memory tile over the drained ring, and the CTA then stores
+//    row after row of C with consecutive threads on consecutive columns,
+//    applying the epilogue (bias + GELU keeping the pre-activation, bias,
+//    plain store, or GELU backward).
 // Out-of-range rows, columns and K are zero-filled by the tensor loads and
 // masked at the stores.  Every mbarrier wait is bounded: a wait that runs
 // out sets the error word, the kernel still waits (bounded) for its copies
@@ -35,16 +41,27 @@ namespace hx {
 
 namespace {
 
-constexpr int kBM = 128, kBN = 128, kBK = 64, kStages = 4;
-constexpr uint32_t kTileBytes = kBM * kBK * 2;             // 16 KB, also kBN * kBK * 2
+constexpr int kBM = 128, kBN = 128, kStages = 4;
+constexpr uint32_t kTileBytes = kBM * 128;                  // 128 rows of 128 bytes: 64 BF16 or 32 TF32 per row
 constexpr uint32_t kStageBytes = 2 * kTileBytes;           // A + B
 constexpr uint32_t kTmemCols = kBN;                        // FP32 accumulator columns
 constexpr uint32_t kSmemBytes = kStages * kStageBytes + 1024 + 256;  // + 1024-byte alignment + barriers
+static_assert(128 * (kBN + 1) * 4 <= kStages * kStageBytes, "the epilogue tile reuses the ring");
 constexpr uint32_t kPoll = 1u << 22;
 
-// tcgen05.mma instruction descriptor: FP32 accumulator, BF16 A and B, both
-// K-major, N = 128, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kBN >> 3) << 17) | (uint32_t(kBM >> 4) << 24);
+// tcgen05.mma instruction descriptor: FP32 accumulator, A and B both BF16
+// (format 1) or both TF32 (format 2), both K-major, N = 128, M = 128.
+__host__ __device__ constexpr uint32_t idesc_of(uint32_t fmt)
+{
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | (uint32_t(kBN >> 3) << 17) | (uint32_t(kBM >> 4) << 24);
+}
+
+// Tensor maps of up to three operand pairs; the kernel accumulates the sum of
+// their products A_p B_p^T (the terms of a split-precision product).
+struct TcMaps {
+    CUtensorMap a[3];
+    CUtensorMap b[3];
+};
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
@@ -107,10 +124,12 @@ __device__ __forceinline__ float gelu_grad_f(float z)
     return cdf + z * pdf;
 }
 
+template <bool TF32>
 __global__ void __launch_bounds__(128, 1)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M, int N,
-                   int K, TcGemmOut o, int* err)
+    tc_gemm_kernel(const __grid_constant__ TcMaps maps, int M, int N, int K, int npairs, TcGemmOut o, int* err)
 {
+    constexpr int kBK = TF32 ? 32 : 64;  // K elements per 128-byte row
+    constexpr uint32_t kIdesc = idesc_of(TF32 ? 2u : 1u);
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = saddr(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;  // swizzled tiles need 1024-byte alignment
@@ -122,8 +141,11 @@ __global__ void __launch_bounds__(128, 1)
     const uint32_t cslot = tslot + 4u;  // K blocks the MMA thread consumed
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-    const int nk = (K + kBK - 1) / kBK;
+    // 1-D grid, N tiles fastest: the CTAs that share a row block of A run together and read it once from HBM
+    const int ntn = (N + kBN - 1) / kBN;
+    const int m0 = static_cast<int>(blockIdx.x / ntn) * kBM, n0 = static_cast<int>(blockIdx.x % ntn) * kBN;
+    const int nkp = (K + kBK - 1) / kBK;  // K blocks of one operand pair
+    const int nk = nkp * npairs;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -157,8 +179,9 @@ __global__ void __launch_bounds__(128, 1)
             const uint32_t a = base + s * kStageBytes, b = a + kTileBytes;
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full_bar(s)), "r"(kStageBytes)
                          : "memory");
-            tma_load_2d(a, &tmA, kb * kBK, m0, full_bar(s));
-            tma_load_2d(b, &tmB, kb * kBK, n0, full_bar(s));
+            const int p = kb / nkp, x = (kb - p * nkp) * kBK;
+            tma_load_2d(a, &maps.a[p], x, m0, full_bar(s));
+            tma_load_2d(b, &maps.b[p], x, n0, full_bar(s));
             issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0) {
@@ -173,14 +196,21 @@ __global__ void __launch_bounds__(128, 1)
             tc_fence_after();
             const uint32_t a = base + s * kStageBytes, b = a + kTileBytes;
 #pragma unroll
-            for (int k = 0; k < kBK / 16; ++k) {
+            for (int k = 0; k < 4; ++k) {  // 32 bytes of K per instruction (16 BF16 or 8 TF32)
                 const uint64_t da = sw128_desc(a + 32u * k), db = sw128_desc(b + 32u * k);
                 const uint32_t accumulate = (kb > 0 || k > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                    "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
-                    : "memory");
+                if constexpr (TF32)
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                        "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+                        : "memory");
+                else
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                        "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+                        : "memory");
             }
             tc_commit(empty_bar(s));  // the stage is free once these MMAs have read it
         }
@@ -188,11 +218,21 @@ __global__ void __launch_bounds__(128, 1)
         tc_commit(done_bar);  // every MMA issued above has completed
     }
 
-    // ---- epilogue: every warp reads its 32 accumulator lanes
+    // ---- epilogue: the accumulator goes through shared memory (the ring is
+    // free once every MMA has completed and every copy has landed) so that
+    // each row of C is stored by consecutive threads
     const bool done = mbar_wait(done_bar, 0);
     if (!done && threadIdx.x == 0) atomicExch(err, 1);
+    if (warp == 0 && lane == 0) {
+        int consumed;
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(consumed) : "r"(cslot) : "memory");
+        for (int kb = consumed; kb < issued; ++kb) mbar_wait(full_bar(kb % kStages), (kb / kStages) & 1);
+    }
     tc_fence_after();
-    const int row = m0 + warp * 32 + lane;
+    __syncthreads();
+    float* stile = reinterpret_cast<float*>(smem_raw + (base - raw));  // [128][kBN + 1]
+    constexpr int kLd = kBN + 1;
+    const int trow = warp * 32 + lane;
     for (int c0 = 0; c0 < kBN; c0 += 16) {
         uint32_t v[16];
         asm volatile(
@@ -202,19 +242,24 @@ __global__ void __launch_bounds__(128, 1)
               "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
             : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (!done || row >= M) continue;
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) {
-            const int col = n0 + c0 + jj;
-            if (col >= N) break;
-            const float val = __uint_as_float(v[jj]);
+        for (int jj = 0; jj < 16; ++jj) stile[trow * kLd + c0 + jj] = __uint_as_float(v[jj]);
+    }
+    __syncthreads();
+    const int col = n0 + static_cast<int>(threadIdx.x);  // kBN == blockDim.x
+    if (done && col < N) {
+        const float bias = (o.kind == kTcEpiBiasGelu || o.kind == kTcEpiBias) ? o.bias[col] : 0.0f;
+        for (int rr = 0; rr < kBM; ++rr) {
+            const int row = m0 + rr;
+            if (row >= M) break;
+            const float val = stile[rr * kLd + threadIdx.x];
             const long long off = static_cast<long long>(row) * o.ldo + col;
             if (o.kind == kTcEpiBiasGelu) {
-                const float z = val + o.bias[col];
+                const float z = val + bias;
                 o.outf[off] = z;
                 static_cast<__nv_bfloat16*>(o.outh)[off] = __float2bfloat16(gelu_f(z));
             } else if (o.kind == kTcEpiBias) {
-                o.outf[off] = val + o.bias[col];
+                o.outf[off] = val + bias;
             } else if (o.kind == kTcEpiStore) {
                 o.outf[off] = val;
             } else {
@@ -223,13 +268,6 @@ __global__ void __launch_bounds__(128, 1)
                 if (o.outf) o.outf[off] = g;
             }
         }
-    }
-
-    // ---- copies still in flight after a wait that ran out land before exit
-    if (warp == 0 && lane == 0) {
-        int consumed;
-        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(consumed) : "r"(cslot) : "memory");
-        for (int kb = consumed; kb < issued; ++kb) mbar_wait(full_bar(kb % kStages), (kb / kStages) & 1);
     }
     tc_fence_before();
     __syncthreads();
@@ -269,48 +307,123 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-// Tensor map of a row-major BF16 matrix [rows x cols] (leading dimension ld),
-// boxes of 128 rows x 64 columns in the 128-byte swizzled layout.
-bool make_map(CUtensorMap* map, const void* ptr, int rows, int cols, int ld)
+// Tensor map of a row-major matrix [rows x cols] (leading dimension ld) of
+// BF16 or FP32 (read as TF32) elements, boxes of 128 rows x 128 bytes in the
+// 128-byte swizzled layout.
+bool make_map(CUtensorMap* map, const void* ptr, int rows, int cols, int ld, bool fp32)
 {
     auto fn = encode_fn();
     if (!fn) return false;
+    const int esize = fp32 ? 4 : 2;
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
-    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2};
-    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kBK), static_cast<cuuint32_t>(kBM)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * esize};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(128 / esize), static_cast<cuuint32_t>(kBM)};
     const cuuint32_t estr[2] = {1, 1};
-    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    return fn(map, fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr),
+              dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-}  // namespace
-
-bool tc_gemm_eligible(const void* A, int lda, const void* B, int ldb)
+template <bool TF32>
+bool configure()
 {
-    return (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (reinterpret_cast<uintptr_t>(B) % 16 == 0) && lda % 8 == 0 &&
-           ldb % 8 == 0 && encode_fn() != nullptr;
-}
-
-bool tc_gemm(int M, int N, int K, const void* A, int lda, const void* B, int ldb, const TcGemmOut& o, int* err,
-             cudaStream_t s)
-{
-    if (M <= 0 || N <= 0 || K <= 0 || !tc_gemm_eligible(A, lda, B, ldb)) return false;
     static bool configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return false;
     if (!configured[dev]) {
-        if (cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(tc_gemm_kernel<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kSmemBytes)) != cudaSuccess)
             return false;
         configured[dev] = true;
     }
-    CUtensorMap ma, mb;
-    if (!make_map(&ma, A, M, K, lda) || !make_map(&mb, B, N, K, ldb)) return false;
-    const dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
-    tc_gemm_kernel<<<grid, 128, kSmemBytes, s>>>(ma, mb, M, N, K, o, err);
     return true;
+}
+
+bool eligible(const void* A, int lda, const void* B, int ldb, int esize)
+{
+    const int align = 16 / esize;  // leading dimensions: multiples of 16 bytes
+    return (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (reinterpret_cast<uintptr_t>(B) % 16 == 0) &&
+           lda % align == 0 && ldb % align == 0 && encode_fn() != nullptr;
+}
+
+}  // namespace
+
+bool tc_gemm_eligible(const void* A, int lda, const void* B, int ldb) { return eligible(A, lda, B, ldb, 2); }
+
+bool tc_gemm_ready(bool tf32) { return encode_fn() != nullptr && (tf32 ? configure<true>() : configure<false>()); }
+
+bool tc_gemm(int M, int N, int K, const void* A, int lda, const void* B, int ldb, const TcGemmOut& o, int* err,
+             cudaStream_t s)
+{
+    const TcPair pair{A, lda, B, ldb};
+    return tc_gemm_sum(M, N, K, 1, &pair, false, o, err, s);
+}
+
+bool tc_gemm_sum(int M, int N, int K, int npairs, const TcPair* pairs, bool tf32, const TcGemmOut& o, int* err,
+                 cudaStream_t s)
+{
+    if (M <= 0 || N <= 0 || K <= 0 || npairs < 1 || npairs > 3) return false;
+    for (int p = 0; p < npairs; ++p)
+        if (!eligible(pairs[p].A, pairs[p].lda, pairs[p].B, pairs[p].ldb, tf32 ? 4 : 2)) return false;
+    if (!(tf32 ? configure<true>() : configure<false>())) return false;
+    TcMaps maps;
+    for (int p = 0; p < npairs; ++p)
+        if (!make_map(&maps.a[p], pairs[p].A, M, K, pairs[p].lda, tf32) ||
+            !make_map(&maps.b[p], pairs[p].B, N, K, pairs[p].ldb, tf32))
+            return false;
+    const long long tiles = static_cast<long long>((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM);
+    if (tiles > 0x7fffffffll) return false;
+    const dim3 grid(static_cast<unsigned>(tiles));
+    if (tf32)
+        tc_gemm_kernel<true><<<grid, 128, kSmemBytes, s>>>(maps, M, N, K, npairs, o, err);
+    else
+        tc_gemm_kernel<false><<<grid, 128, kSmemBytes, s>>>(maps, M, N, K, npairs, o, err);
+    return true;
+}
+
+// TF32 split of FP32 values: hi = x rounded to TF32 (10 mantissa bits, to
+// nearest, ties away from zero), lo = (x - hi) rounded the same way; both are
+// exact TF32 values, so the products do not depend on how the tensor cores
+// treat the low mantissa bits of an FP32 operand.  |x - hi - lo| <= 2^-22 |x|,
+// and A B ~ A_hi B_hi + A_hi B_lo + A_lo B_hi leaves out terms of that order.
+__device__ __forceinline__ float tf32_round(float v)
+{
+    return __uint_as_float((__float_as_uint(v) + 0x1000u) & 0xFFFFE000u);
+}
+
+__global__ void tf32_split_kernel(const float* __restrict__ x, float* __restrict__ hi, float* __restrict__ lo,
+                                  long long n)
+{
+    const long long n4 = n >> 2;
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+    float4* h4 = reinterpret_cast<float4*>(hi);
+    float4* l4 = reinterpret_cast<float4*>(lo);
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n4; i += stride) {
+        const float4 v = __ldcs(x4 + i);
+        float4 h, l;
+        h.x = tf32_round(v.x);
+        h.y = tf32_round(v.y);
+        h.z = tf32_round(v.z);
+        h.w = tf32_round(v.w);
+        l.x = tf32_round(v.x - h.x);
+        l.y = tf32_round(v.y - h.y);
+        l.z = tf32_round(v.z - h.z);
+        l.w = tf32_round(v.w - h.w);
+        h4[i] = h;
+        l4[i] = l;
+    }
+    for (long long i = 4 * n4 + blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+        const float h = tf32_round(x[i]);
+        hi[i] = h;
+        lo[i] = tf32_round(x[i] - h);
+    }
+}
+
+void launch_tf32_split(const float* x, float* hi, float* lo, long long n, cudaStream_t s)
+{
+    tf32_split_kernel<<<148 * 8, 256, 0, s>>>(x, hi, lo, n);
 }
 
 void launch_transpose_bf16(const void* in, int rows, int cols, int ld_in, void* out, int ld_out, cudaStream_t s)

@@ -378,6 +378,39 @@ def random_hermitian_csr(dim: int, per_row: int, seed: int, scale: float = 1.0):
     return np.array(ptr, np.int32), np.array(col, np.int32), np.array(val, np.complex128)
 
 
+def dense_hermitian(dim: int, seed: int, scale: float = 1.0) -> np.ndarray:
+    """Seeded dense complex Hermitian matrix: entries (r <= c) from splitmix64
+    uniforms in (-scale, scale), real diagonal, divided by sqrt(dim) so the
+    spectrum stays O(scale) as dim grows."""
+    rng = SplitMix64(seed)
+    m = np.zeros((dim, dim), np.complex128)
+    for r in range(dim):
+        m[r, r] = 2.0 * rng.uniform() - 1.0
+        for c in range(r + 1, dim):
+            v = complex(2.0 * rng.uniform() - 1.0, 2.0 * rng.uniform() - 1.0)
+            m[r, c] = v
+            m[c, r] = v.conjugate()
+    return m * (scale / math.sqrt(dim))
+
+
+def dense_h_problem(n_spins: int, seed: int, eps: float = 0.5, h: float = 0.5, depth: int = 2, K: int = 1,
+                    n_baths: int | None = None, lam: float = 0.1, gamma: float = 1.0, temperature: float = 1.0,
+                    dt: float = 0.005) -> Problem:
+    """Spin glass with a dense perturbation: H = E + h sum_i sx_i + eps G, G a
+    seeded dense Hermitian matrix (dense_hermitian), passed as a CSR with all
+    d^2 entries; sz baths on the first n_baths spins (all by default)."""
+    base = spin_glass(n_spins, seed, h=h, lam=lam, gamma=gamma, temperature=temperature, K=K, depth=depth, dt=dt)
+    d = base.dim
+    m = base.h_dense() + dense_hermitian(d, seed * 7919 + 1, eps)
+    nb = n_spins if n_baths is None else n_baths
+    ptr = np.arange(0, d * d + 1, d, dtype=np.int32)
+    col = np.tile(np.arange(d, dtype=np.int32), d)
+    val = m.reshape(-1).copy()
+    return Problem(dim=d, h_diag=np.real(np.diag(m)).copy(), h_flip=np.zeros(n_spins), baths=base.baths[:nb],
+                   max_depth=depth + 1, dt=dt, name=f"dense_h_n{n_spins}_L{depth}_K{K}_b{nb}",
+                   meta={"seed": seed, "eps": eps, "h": h, "depth": depth}, h_csr_explicit=(ptr, col, val))
+
+
 def sparse_problem(n_spins: int, seed: int, depth: int = 2, K: int = 1, lam: float = 0.1, gamma: float = 1.0,
                    temperature: float = 1.0, dt: float = 0.01, per_row: int = 3) -> Problem:
     """A general sparse instance (System::from_sparse style): random sparse

@@ -92,7 +92,7 @@ typedef struct hx_problem {
     double time_step;           /* dt (Param::Step) */
     uint32_t integration_order; /* Taylor order (Param::IntegrationNum), 1..8 */
     uint32_t precision;         /* HX_PRECISION_DOUBLE or HX_PRECISION_MIXED */
-    uint32_t flags;             /* 0 or HX_FLAG_FULL_STATE */
+    uint32_t flags;             /* 0, HX_FLAG_FULL_STATE, HX_FLAG_DENSE_H */
     const hx_csr* h_csr;        /* or NULL; a general Hermitian H, in place of h_diag / h_flip */
 } hx_problem;
 
@@ -113,6 +113,15 @@ typedef struct hx_problem {
  * slabs; hx_ctx_write_state then rejects non-Hermitian ADOs.  This flag keeps
  * full slabs on the device, for general (non-Hermitian) states. */
 #define HX_FLAG_FULL_STATE 1u
+/* hx_problem.flags: evaluate the Hamiltonian commutator -i[H, u_n] of every
+ * ADO as matrix products on the tensor cores (tcgen05, TF32 operands in a
+ * 3-term split product, FP32 accumulation), for a general dense Hermitian H
+ * (h_csr with any number of entries per row, or h_diag / h_flip).  Needs
+ * HX_PRECISION_MIXED, HX_FLAG_FULL_STATE, diagonal coupling operators and
+ * 128 <= dim <= 1024; the states must be Hermitian (hx_ctx_write_state
+ * checks).  No counterpart in the reference, whose H is diagonal
+ * (src/legacy_compile_options.h:3) or applied as a sparse product. */
+#define HX_FLAG_DENSE_H 2u
 
 typedef struct hx_info {
     uint32_t dim;
@@ -135,6 +144,7 @@ typedef struct hx_info {
 #define HX_PATH_FLIP 3u     /* comm_kernel + combine_kernel: couplings with spin flips */
 #define HX_PATH_CSR 4u      /* csr_comm_kernel + csr_combine_kernel: general sparse operators */
 #define HX_PATH_SMALL 5u    /* small_kernel: d <= 16 with sigma_z couplings (batched neighbour gathers) */
+#define HX_PATH_DENSE 6u    /* HX_FLAG_DENSE_H: tf32_split_kernel + tc_gemm_kernel (Y = X H) + band kernels */
 
 /* Profiling counters (replaces src/library/backend_profiling.cpp:9-137). */
 typedef struct hx_counters {

@@ -100,12 +100,19 @@ def test_hermitian_packed_layout_is_a_bijection(d):
     np.testing.assert_array_equal(capi.unpack_herm(pk, d), x)
 
 
-def test_full_state_flag_is_the_only_flag():
+def test_unknown_flags_and_dense_h_preconditions():
     p = S.spin_glass(2, seed=1, depth=2, K=1)
-    prob, keep = capi._problem_struct(p, flags=2)
+    prob, keep = capi._problem_struct(p, flags=4)
     h = C.c_void_p()
     rc = capi.lib().hx_ctx_create(C.byref(prob), C.byref(h))
     assert rc == 6 and "flags" in capi.lib().hx_last_error().decode()  # InvalidRuntimeOption, no device call
+    # HX_FLAG_DENSE_H needs mixed precision and full slabs: refused on the host
+    p = S.spin_glass(7, seed=1, depth=2, K=1)
+    for prec, flags in ((capi.PRECISION_DOUBLE, capi.FLAG_DENSE_H | capi.FLAG_FULL_STATE),
+                        (capi.PRECISION_MIXED, capi.FLAG_DENSE_H)):
+        prob, keep = capi._problem_struct(p, precision=prec, flags=flags)
+        rc = capi.lib().hx_ctx_create(C.byref(prob), C.byref(h))
+        assert rc == 10 and "HX_FLAG_DENSE_H" in capi.lib().hx_last_error().decode()  # UnsupportedExecution
 
 
 def test_energy_trace_writer_matches_the_reference_format(tmp_path, golden):
