@@ -42,6 +42,11 @@ CONFIGS = {
     # mixed precision: N=8 (d=256), h=0.5, Pade K=1 (16 modes), depth L=3 -> 969 ADOs, dt=0.005, 500 steps
     "c3": dict(n=8, depth=3, K=1, h=0.5, dt=0.005, seed=2027, mixed=True, error_steps=500,
                workload="spin_glass_d256_L3_K1_969ados_complex64_mixed"),
+    # dense H on the tensor cores: the C3 hierarchy (N=8, d=256, K=1, L=3: 969 ADOs, dt=0.005) with
+    # H = E + h sum sx + 0.5 G, G a seeded dense Hermitian matrix (every entry non-zero); complex64
+    # hierarchy, rho_0 in FP64, commutator as 3-term TF32 split products; error against the FP64 CSR path
+    "c3dense": dict(n=8, depth=3, K=1, h=0.5, eps=0.5, dt=0.005, seed=2027, dense=True, error_steps=100,
+                    workload="dense_h_d256_L3_K1_969ados_complex64_tf32x3"),
     # learned closure: N=5 (d=32), K=2 (15 modes), L=2 + MLP closure of tier 3; trained on 64 seeds of plain
     # L=5 FP64 runs (dt=0.01, 1000 steps), tested on 16 held-out seeds against plain L=5
     "c5": dict(n=5, K=2, h=1.0, dt=0.01, closure=True, coarse_depth=2, fine_depth=5, train_seeds=64,
@@ -56,6 +61,9 @@ CONFIGS = {
 def make_problem(cfg: dict, rank: int = 0):
     if cfg.get("legacy"):
         return S.legacy_spin_glass(cfg["dim"])
+    if cfg.get("dense"):
+        return S.dense_h_problem(cfg["n"], seed=cfg["seed"] + rank, eps=cfg["eps"], h=cfg["h"], depth=cfg["depth"],
+                                 K=cfg["K"], dt=cfg["dt"])
     return S.spin_glass(cfg["n"], seed=cfg["seed"] + rank, depth=cfg["depth"], K=cfg["K"], h=cfg["h"],
                         dt=cfg["dt"])
 
@@ -845,6 +853,167 @@ def run_mixed(args, cfg: dict) -> None:
     print(json.dumps(line), flush=True)
 
 
+def load_tensor_peak() -> tuple[float, str]:
+    """Dense TF32 tensor peak in TFLOP/s: half the measured BF16 GEMM rate (the
+    TF32 tensor rate is half the BF16 rate on this part), else half the
+    fallback BF16 figure."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return 0.5 * float(json.load(f)["bf16_tflops"]), "measured bf16_tflops / 2 (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError):
+        return 0.5 * 1590.0, "fallback 1590 TFLOP/s bf16 / 2"
+
+
+def run_dense(args, cfg: dict) -> None:
+    """Dense H on the tensor cores (HX_FLAG_DENSE_H) against the plain FP64
+    propagator for the same H (the CSR path, the only FP64 path for a dense
+    H) on the same GPU.  The roofline is the tensor one: the GEMM kernel alone
+    (hx_ctx_dense_product, parts = 2) timed with CUDA events, algorithmic FLOPs
+    8 H d^3 per launch (the complex product X H_off of every ADO) and executed
+    FLOPs 3x that (the TF32 split)."""
+    import torch
+
+    from helix_b200 import capi
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return  # one hierarchy: the comparison runs on one GPU
+    p = make_problem(cfg, 0)
+    stream = torch.cuda.Stream()
+    H, d = p.hierarchy_size(), p.dim
+
+    def events_ms(fn) -> float:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1)
+
+    ctx = capi.Context(p, precision="mixed", dense_h=True)
+    ctx.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        ctx.step(1)
+    ctx.sync()
+    c0 = ctx.counters()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = events_ms(lambda: ctx.step(args.steps))
+    clk = clocks.stop()
+    launches = int(ctx.counters().kernel_launches - c0.kernel_launches)
+    info = ctx.get_info()
+    # the GEMM alone, and the split alone, on the current state
+    reps = 20
+    ctx.dense_product(2, 3)
+    gemm_ms = events_ms(lambda: ctx.dense_product(reps, 2)) / reps
+    split_ms = events_ms(lambda: ctx.dense_product(reps, 1)) / reps
+    ctx.close()
+    value = H * args.steps / (ms / 1000.0)
+
+    # cuBLAS TF32 on one of the three products of the same shape, for scale (not on the product path)
+    torch.backends.cuda.matmul.allow_tf32 = True
+    a = torch.randn(H * d, 2 * d, device="cuda")
+    b = torch.randn(2 * d, 2 * d, device="cuda")
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            a @ b
+        cublas_ms = events_ms(lambda: [a @ b for _ in range(reps)]) / reps
+    del a, b
+
+    # plain FP64 propagator for the same dense H (CSR path) and the error against it
+    c64 = capi.Context(p)
+    c64.set_stream(stream.cuda_stream)
+    c64.step(1)
+    c64.sync()
+    k64 = 2
+    ms64 = events_ms(lambda: c64.step(k64)) / k64
+    c64.close()
+
+    def trace_distance(x, y):
+        m = x - y
+        return 0.5 * float(np.sum(np.abs(np.linalg.eigvalsh(0.5 * (m + m.conj().T)))))
+
+    n_err = cfg["error_steps"]
+    c64 = capi.Context(p)
+    cm = capi.Context(p, precision="mixed", dense_h=True)
+    td, en_err, tr_err = [], [], []
+    for _ in range(n_err // 10):
+        r64, e64 = c64.step_trace(10)
+        rm, em = cm.step_trace(10)
+        td.append(trace_distance(rm[-1], r64[-1]))
+        en_err.append(float(np.max(np.abs(em - e64))))
+        tr_err.append(abs(float(np.trace(rm[-1]).real) - 1.0))
+    c64.close()
+    cm.close()
+
+    # end to end through the C ABI: state upload from host, steps with rho_0(t) and <H>(t), final rho_0
+    pinned = torch.empty(H * d * d * 2, dtype=torch.float64, pin_memory=True)
+    host_state = pinned.numpy().view(np.complex128).reshape(H, d, d)
+    host_state[:] = 0
+    host_state[0] = S.initial_rho0(d)
+    rho_trace = torch.empty(args.steps * d * d * 2, dtype=torch.float64, pin_memory=True).numpy()
+    en_trace = np.zeros(args.steps)
+    ctx = capi.Context(p, precision="mixed", dense_h=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.set_state(host_state)
+    ctx.step_trace_into(args.steps, rho_trace, en_trace)
+    ctx.rho0()
+    e2e_sec = time.perf_counter() - t0
+    ctx.close()
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        # one full step of the same H and baths with a depth-1 hierarchy (17 ADOs), per ADO
+        from oracle import oracle as O
+        q = make_problem(dict(cfg, depth=1), 0)
+        o = O.Oracle(q)
+        t0 = time.perf_counter()
+        o.run(1)
+        sec = time.perf_counter() - t0
+        o.close()
+        cpu = {"value": q.hierarchy_size() / sec, "unit": UNIT, "cores": O.threads(), "kind": "port",
+               "sample": f"1 full step of the same H and baths at depth 1 ({q.hierarchy_size()} ADOs), "
+                         "FP64 oracle (CSR H), OpenMP; per-ADO cost does not depend on the depth"}
+    alg = 8.0 * H * d ** 3
+    tpeak, tpeak_src = load_tensor_peak()
+    achieved = alg / (gemm_ms / 1000.0) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 state, tf32x3 products, f32 accumulate (rho_0 f64)", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "ados": H, "dim": d, "modes": p.modes, "depth_L": p.max_depth - 1,
+                   "dt": p.dt, "h_nnz_per_row": d, "integrator": "RK4 (4-term Taylor, Horner form)",
+                   "parallelism": "single", "l2": f"inputs larger than L2 (state {H * d * d * 8 / 1e9:.3f} GB complex64)"},
+        "plain_fp64_same_gpu": {"value": H / (ms64 / 1000.0), "ms_per_step": ms64, "path": "csr (FP64)",
+                                "speedup": value / (H / (ms64 / 1000.0))},
+        "error_vs_fp64": {"trace_distance_max": max(td), "trace_distance_final": td[-1],
+                          "energy_abs_max": max(en_err), "trace_abs_max": max(tr_err), "steps": n_err, "every": 10},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": tpeak, "unit": "TFLOP/s",
+                     "frac": achieved / tpeak, "traffic": profiled_traffic(args.config, "tc_gemm_kernel"),
+                     "peak_source": tpeak_src, "kernel": "tc_gemm_kernel<tf32, 256>",
+                     "algorithmic_flops_per_launch": alg, "executed_flops_per_launch": 3 * alg,
+                     "executed_tflops": 3 * achieved, "launch_ms": gemm_ms,
+                     "cublas_tf32_one_product_ms": cublas_ms,
+                     "cublas_tf32_tflops": alg / (cublas_ms / 1000.0) / 1e12,
+                     "split_kernel_ms": split_ms},
+        "e2e": {"value": H * args.steps / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": H * d * d * 16 / args.steps,
+                "d2h_bytes_per_step": d * d * 16 + 24,
+                "path": "hx_ctx_write_state + hx_ctx_step_trace (rho0, <H> per step) + hx_ctx_read_rho0"},
+        "gpu_launches": launches,
+        "kernels_per_step": int(info.kernels_per_step),
+        "clocks": clk,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
 def run_closure(args, cfg: dict) -> None:
     """Learned closure: L=2 hierarchy + MLP closure of tier 3 against the plain
     L=5 run (the reference solution) and the plain truncated L=2 run, on held-out seeds.
@@ -987,6 +1156,8 @@ def main() -> None:
         run_batch(args, cfg)
     elif cfg.get("mixed"):
         run_mixed(args, cfg)
+    elif cfg.get("dense"):
+        run_dense(args, cfg)
     elif cfg.get("closure"):
         run_closure(args, cfg)
     else:

@@ -34,7 +34,7 @@ EXPORTS = [
     "hx_seeded_couplings", "hx_ctx_create", "hx_ctx_destroy", "hx_ctx_set_stream", "hx_ctx_get_stream",
     "hx_ctx_info", "hx_ctx_counters", "hx_ctx_step", "hx_ctx_step_trace", "hx_ctx_sync",
     "hx_ctx_read_rho0", "hx_ctx_observables", "hx_ctx_read_state", "hx_ctx_write_state",
-    "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_check_finite", "hx_rhs_noalloc",
+    "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_dense_product", "hx_ctx_check_finite", "hx_rhs_noalloc",
     "hx_ctx_save_snapshot", "hx_ctx_load_snapshot", "hx_write_energy_trace",
     "hx_batch_create", "hx_batch_destroy", "hx_batch_set_stream", "hx_batch_info", "hx_batch_tune",
     "hx_batch_step", "hx_batch_sync", "hx_batch_read_rho0",
@@ -148,6 +148,7 @@ def lib():
             L.hx_ctx_read_rho0.argtypes = [vp, vp, u64]
             L.hx_ctx_observables.argtypes = [vp, dp, dp, dp]
             L.hx_ctx_read_state.argtypes = [vp, vp, u64]
+            L.hx_ctx_dense_product.argtypes = [vp, u32, u32]
             L.hx_ctx_write_state.argtypes = [vp, vp, u64]
             L.hx_ctx_state_device_ptr.argtypes = [vp, C.POINTER(vp)]
             L.hx_ctx_rhs.argtypes = [vp, vp, u64]
@@ -416,6 +417,10 @@ class Context:
         s = np.ascontiguousarray(s, np.complex128)
         assert s.size == self.size * self.dim * self.dim
         _check(lib().hx_ctx_write_state(self._h, _p(s), 2 * s.size))
+
+    def dense_product(self, count: int = 1, parts: int = 3) -> None:
+        """Enqueue ``count`` tensor-core products of a ``dense_h`` context (parts: 1 split, 2 GEMM, 3 both)."""
+        _check(lib().hx_ctx_dense_product(self._h, C.c_uint32(count), C.c_uint32(parts)))
 
     def rhs(self) -> np.ndarray:
         out = np.zeros((self.size, self.dim, self.dim), np.complex128)

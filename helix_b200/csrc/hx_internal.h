@@ -261,8 +261,7 @@ struct Ado0Args {
     const double* ent_wa;
     int M, J, logd;
     int herm;                // 1: the slabs (and diag) are Hermitian-packed
-    const float2* dense_y;   // dense H: Y_0 = X_0 H_off (as in LargeArgs), else nullptr
-    const double2* dense_h;  // dense H: H_off [d][d] in FP64 (the diagonal of the commutator, exactly traceless)
+    const double2* dense_z;  // dense H: Z_0 = X_0 H_off in FP64 ([d][d], from zgemm_kernel), else nullptr
 };
 bool large_supported(int logd, int M, int J);
 template <typename R> bool prepare_large(const LargeArgs<R>& a);  // shared-memory limit; call before capture
@@ -270,6 +269,8 @@ template <typename R>
 bool launch_large(const LargeArgs<R>& a, const C2<R>* u, const C2<R>* rho, C2<R>* out, double alpha, int base_kind,
                   cudaStream_t s);
 template <typename R> void launch_large_upterm(const LargeUpArgs<R>& a, const C2<R>* u, C2<R>* U, cudaStream_t s);
+// Z = X H for one d x d complex pair in FP64, row-major (d = 2^logd >= 32): ADO 0 of a dense-H stage
+void launch_zgemm(const double2* x, const double2* h, double2* z, int logd, cudaStream_t s);
 void launch_ado0(const Ado0Args& a, const double2* u0, const float2* u, const double2* rho0, double2* out0,
                  float2* out32, double alpha, int base_kind, cudaStream_t s);
 void launch_d2f(const double2* in, float2* out, long long n, cudaStream_t s);
@@ -432,7 +433,8 @@ struct hx_ctx {
     float* dense_xhi = nullptr;   // [H][d][2d] TF32 split of the stage input
     float* dense_xlo = nullptr;
     float2* dense_y = nullptr;    // [H][d][d] Y_n = X_n H_off (H without its diagonal)
-    double2* dense_h64 = nullptr; // [d][d] H_off in FP64 (ADO 0's diagonal commutator terms)
+    double2* dense_h64 = nullptr; // [d][d] H_off in FP64 (ADO 0's product)
+    double2* dense_z0 = nullptr;  // [d][d] Z_0 = X_0 H_off in FP64
     bool launch_failed = false;   // a stage could not be enqueued (reported by the next error check)
     size_t state_pinned_elems = 0;
     size_t device_bytes = 0;

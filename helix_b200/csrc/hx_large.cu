@@ -70,10 +70,13 @@ __global__ void __launch_bounds__(256, 2)
     R* sH = sV + a.J * D;                                     // [LOGD]
     int* sSlab = reinterpret_cast<int*>(sH + LOGD + 1);       // [2M]
     int* sBath = sSlab + 2 * a.M;                             // [2M]
+    constexpr int RB = BE / D, RBP = RB + 1;                  // rows of the band; padded strip row
+    C* sYT = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(sBath + 2 * a.M) + 15) & ~uintptr_t(15));  // [D][RBP]
 
     const int tid = threadIdx.x;
     const long long n = a.first_ado + static_cast<long long>(blockIdx.x) / NB;
     const long long be = static_cast<long long>(blockIdx.x % NB) * BE;  // band's first element in the slab
+    const int r0 = static_cast<int>(be >> LOGD);                        // band's first row
     const C* un = u + n * D2;
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(l_addr(bar)) : "memory");
@@ -99,9 +102,22 @@ __global__ void __launch_bounds__(256, 2)
         sWc[q] = a.ent_wc[src];
         sWa[q] = a.ent_wa[src];
     }
+    if (a.dense_y) {
+        // dense H: the strip Y_n[c][r0 .. r0 + RB) of every column c (coalesced row pieces, asynchronous
+        // 8-byte copies that overlap the table loads) for the transposed elements Y_cr of this band
+        const C* yn = a.dense_y + n * D2;
+#pragma unroll
+        for (int k = 0; k < BE / T; ++k) {
+            const int i = tid + k * T, cc = i / RB, j = i - cc * RB;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(l_addr(sYT + cc * RBP + j)),
+                         "l"(yn + (static_cast<long long>(cc) << LOGD) + r0 + j)
+                         : "memory");
+        }
+    }
     const R g = static_cast<R>(a.gsum[n]);
     const int slot = a.slot ? a.slot[n] : -1;
     const R alpha = static_cast<R>(alpha_d);
+    if (a.dense_y) asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
     bool ok = false;
     for (uint32_t it = 0; it < kLargeSpin && !ok; ++it) {
@@ -150,8 +166,7 @@ __global__ void __launch_bounds__(256, 2)
             if (a.dense_y) {
                 // -i [H_off, X] = -i (conj(Y_cr) - Y_rc) from the tensor-core product Y = X H_off
                 const int r = static_cast<int>(ge >> LOGD), c = static_cast<int>(ge & (D - 1));
-                const C* yn = a.dense_y + n * D2;
-                const C yrc = __ldg(yn + ge), ycr = __ldg(yn + (static_cast<long long>(c) << LOGD) + r);
+                const C yrc = __ldg(a.dense_y + n * D2 + ge), ycr = sYT[c * RBP + (r - r0)];
                 acc[k0 + kk].x -= yrc.y + ycr.y;
                 acc[k0 + kk].y += yrc.x - ycr.x;
             }
@@ -489,23 +504,12 @@ __global__ void __launch_bounds__(256)
     }
     double ax = t.x * x.x - t.y * x.y + hi;
     double ay = t.x * x.y + t.y * x.x - hr;
-    if (a.dense_y && r != c) {
-        // -i [H_off, X] = -i (conj(Y_cr) - Y_rc) of ADO 0 from the tensor-core product Y = X H_off
-        const float2 yrc = a.dense_y[ge], ycr = a.dense_y[(static_cast<long long>(c) << a.logd) + r];
-        ax -= static_cast<double>(yrc.y) + static_cast<double>(ycr.y);
-        ay += static_cast<double>(yrc.x) - static_cast<double>(ycr.x);
-    } else if (a.dense_y) {
-        // diagonal: -i [H_off, X]_rr = -2 Im z_r, z_r = sum_k X_rk conj(H_rk) (X, H Hermitian), in FP64 so
-        // that the commutator stays traceless (sum_r Im z_r = Im Tr(X H) = 0) to FP64 rounding
-        const double2* xr = u0 + (static_cast<long long>(r) << a.logd);
-        const double2* hr_row = a.dense_h + (static_cast<long long>(r) << a.logd);
-        double z0 = 0.0, z1 = 0.0;
-        for (int k = 0; k < D; k += 2) {
-            const double2 x0 = xr[k], h0 = hr_row[k], x1 = xr[k + 1], h1 = hr_row[k + 1];
-            z0 += x0.y * h0.x - x0.x * h0.y;
-            z1 += x1.y * h1.x - x1.x * h1.y;
-        }
-        ax -= 2.0 * (z0 + z1);
+    if (a.dense_z) {
+        // -i [H_off, X] = -i (conj(Z_cr) - Z_rc) of ADO 0 from its FP64 product Z = X H_off (X, H Hermitian);
+        // the diagonal terms -2 Im Z_rr sum to -2 Im Tr(X H_off) = 0, so the commutator stays traceless
+        const double2 zrc = a.dense_z[ge], zcr = a.dense_z[(static_cast<long long>(c) << a.logd) + r];
+        ax -= zrc.y + zcr.y;
+        ay += zrc.x - zcr.x;
     }
     const int Q = a.ent_count[0];
     for (int q = 0; q < Q; ++q) {
@@ -527,6 +531,48 @@ __global__ void __launch_bounds__(256)
     out32[ge] = make_float2(static_cast<float>(o.x), static_cast<float>(o.y));
 }
 
+// Z = X H, d x d complex FP64 (ADO 0 of a dense-H stage): 32 x 32 output
+// tiles, K staged through shared memory 16 at a time; each thread keeps four
+// outputs of one column.  d^3 complex multiply-adds, a few microseconds at
+// d = 256.
+__global__ void __launch_bounds__(256) zgemm_kernel(const double2* __restrict__ x, const double2* __restrict__ h,
+                                                    double2* __restrict__ z, int logd)
+{
+    constexpr int TM = 32, TN = 32, TK = 16;
+    __shared__ double2 sa[TM][TK + 1];
+    __shared__ double2 sb[TK][TN + 1];
+    const int D = 1 << logd;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double2 acc[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[j] = make_double2(0.0, 0.0);
+    for (int k0 = 0; k0 < D; k0 += TK) {
+        for (int i = threadIdx.x; i < TM * TK; i += 256) {
+            const int rr = i / TK, kk = i - rr * TK;
+            sa[rr][kk] = x[(static_cast<long long>(m0 + rr) << logd) + k0 + kk];
+        }
+        for (int i = threadIdx.x; i < TK * TN; i += 256) {
+            const int kk = i / TN, cc = i - kk * TN;
+            sb[kk][cc] = h[(static_cast<long long>(k0 + kk) << logd) + n0 + cc];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TK; ++kk) {
+            const double2 b = sb[kk][tx];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double2 av = sa[ty + 8 * j][kk];
+                acc[j].x = fma(av.x, b.x, fma(-av.y, b.y, acc[j].x));
+                acc[j].y = fma(av.x, b.y, fma(av.y, b.x, acc[j].y));
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) z[(static_cast<long long>(m0 + ty + 8 * j) << logd) + n0 + tx] = acc[j];
+}
+
 __global__ void d2f_kernel(const double2* __restrict__ in, float2* __restrict__ out, long long n)
 {
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
@@ -542,17 +588,18 @@ __global__ void vec_d2f_kernel(const double* __restrict__ in, float* __restrict_
 }
 
 template <typename R, int LOGD>
-size_t large_smem(int M, int J)
+size_t large_smem(int M, int J, bool dense)
 {
+    const size_t strip = dense ? sizeof(C2<R>) * (1 << LOGD) * (4096 / (1 << LOGD) + 1) + 16 : 0;
     return 4096 * sizeof(C2<R>) + 16 + sizeof(double) * 4 * M + sizeof(R) * (J * (1 << LOGD) + LOGD + 1) +
-           sizeof(int) * 4 * M + 16;
+           sizeof(int) * 4 * M + 16 + strip;
 }
 
 template <typename R, int LOGD>
 bool launch_t(const LargeArgs<R>& a, const C2<R>* u, const C2<R>* rho, C2<R>* out, double alpha, int base,
               cudaStream_t s, bool launch)
 {
-    const size_t smem = large_smem<R, LOGD>(a.M, a.J);
+    const size_t smem = large_smem<R, LOGD>(a.M, a.J, a.dense_y != nullptr);
     if (smem > 227 * 1024) return false;
     static size_t configured[64] = {};
     int dev = 0;
@@ -629,6 +676,12 @@ template bool launch_large<float>(const LargeArgs<float>&, const float2*, const 
                                   cudaStream_t);
 template void launch_large_upterm<double>(const LargeUpArgs<double>&, const double2*, double2*, cudaStream_t);
 template void launch_large_upterm<float>(const LargeUpArgs<float>&, const float2*, float2*, cudaStream_t);
+
+void launch_zgemm(const double2* x, const double2* h, double2* z, int logd, cudaStream_t s)
+{
+    const unsigned nt = 1u << (logd - 5);
+    zgemm_kernel<<<dim3(nt, nt), 256, 0, s>>>(x, h, z, logd);
+}
 
 void launch_ado0(const Ado0Args& a, const double2* u0, const float2* u, const double2* rho0, double2* out0,
                  float2* out32, double alpha, int base_kind, cudaStream_t s)

@@ -6,14 +6,14 @@
 // stage (hx_ctx.cu; TF32, the three pairs of a split product, plain store).
 // No counterpart in the reference.
 //
-// One CTA of four warps computes a 128 x 128 tile of C (1-D grid, N tiles
-// fastest):
-//  * warp 0 allocates 128 tensor-memory columns (the 128 x 128 FP32
+// One CTA of four warps computes a 128 x BN tile of C (BN = 256 when N >=
+// 256, else 128; 1-D grid, N tiles fastest):
+//  * warp 0 allocates BN tensor-memory columns (the 128 x BN FP32
 //    accumulator, one lane per row) and its lane 0 streams the K blocks of
-//    every pair (128 rows x 128 bytes of A and of B: 64 BF16 or 32 TF32, 16 KB
-//    each) into a 4-stage shared-memory ring with TMA tensor loads in the
-//    128-byte swizzled layout;
-//  * lane 0 of warp 1 issues tcgen05.mma (M = 128, N = 128, 32 bytes of K per
+//    every pair (128 bytes of each of the 128 rows of A and BN rows of B: 64
+//    BF16 or 32 TF32) into a 192 KB shared-memory ring (6 stages at BN = 128,
+//    4 at 256) with TMA tensor loads in the 128-byte swizzled layout;
+//  * lane 0 of warp 1 issues tcgen05.mma (M = 128, N = BN, 32 bytes of K per
 //    instruction: K = 16 BF16 or 8 TF32; four per K block, the shared-memory
 //    descriptor advanced by 32 bytes inside the swizzle atom) and returns each
 //    stage to the producer with tcgen05.commit on that stage's mbarrier;
@@ -41,19 +41,28 @@ namespace hx {
 
 namespace {
 
-constexpr int kBM = 128, kBN = 128, kStages = 4;
-constexpr uint32_t kTileBytes = kBM * 128;                  // 128 rows of 128 bytes: 64 BF16 or 32 TF32 per row
-constexpr uint32_t kStageBytes = 2 * kTileBytes;           // A + B
-constexpr uint32_t kTmemCols = kBN;                        // FP32 accumulator columns
-constexpr uint32_t kSmemBytes = kStages * kStageBytes + 1024 + 256;  // + 1024-byte alignment + barriers
-static_assert(128 * (kBN + 1) * 4 <= kStages * kStageBytes, "the epilogue tile reuses the ring");
+constexpr int kBM = 128;
+constexpr uint32_t kRowBytes = 128;  // one K block: 128 bytes of every row (64 BF16 or 32 TF32)
 constexpr uint32_t kPoll = 1u << 22;
 
+// Tile of BN = 128 or 256 columns: stage bytes (A then B), ring depth and
+// dynamic shared memory (ring + 1024-byte alignment + barriers).
+template <int BN>
+struct TileCfg {
+    static constexpr uint32_t kABytes = kBM * kRowBytes;
+    static constexpr uint32_t kStageBytes = kABytes + BN * kRowBytes;
+    static constexpr int kStages = BN == 128 ? 6 : 4;  // a 192 KB ring either way
+    static constexpr uint32_t kRing = kStages * kStageBytes;
+    static constexpr uint32_t kSmem = kRing + 1024 + 256;
+    static_assert(kBM * (BN + 1) * 4 <= kRing, "the epilogue tile reuses the ring");
+    static_assert(kSmem <= 227 * 1024, "shared memory per CTA");
+};
+
 // tcgen05.mma instruction descriptor: FP32 accumulator, A and B both BF16
-// (format 1) or both TF32 (format 2), both K-major, N = 128, M = 128.
-__host__ __device__ constexpr uint32_t idesc_of(uint32_t fmt)
+// (format 1) or both TF32 (format 2), both K-major, M = 128, N = BN.
+__host__ __device__ constexpr uint32_t idesc_of(uint32_t fmt, int bn)
 {
-    return (1u << 4) | (fmt << 7) | (fmt << 10) | (uint32_t(kBN >> 3) << 17) | (uint32_t(kBM >> 4) << 24);
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | (uint32_t(bn >> 3) << 17) | (uint32_t(kBM >> 4) << 24);
 }
 
 // Tensor maps of up to three operand pairs; the kernel accumulates the sum of
@@ -124,16 +133,19 @@ __device__ __forceinline__ float gelu_grad_f(float z)
     return cdf + z * pdf;
 }
 
-template <bool TF32>
+template <bool TF32, int BN>
 __global__ void __launch_bounds__(128, 1)
     tc_gemm_kernel(const __grid_constant__ TcMaps maps, int M, int N, int K, int npairs, TcGemmOut o, int* err)
 {
+    using Cfg = TileCfg<BN>;
+    constexpr int kStages = Cfg::kStages;
+    constexpr uint32_t kStageBytes = Cfg::kStageBytes;
     constexpr int kBK = TF32 ? 32 : 64;  // K elements per 128-byte row
-    constexpr uint32_t kIdesc = idesc_of(TF32 ? 2u : 1u);
+    constexpr uint32_t kIdesc = idesc_of(TF32 ? 2u : 1u, BN);
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = saddr(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;  // swizzled tiles need 1024-byte alignment
-    const uint32_t bars = base + kStages * kStageBytes;
+    const uint32_t bars = base + Cfg::kRing;
     auto full_bar = [&](int s) { return bars + 8u * s; };
     auto empty_bar = [&](int s) { return bars + 8u * (kStages + s); };
     const uint32_t done_bar = bars + 8u * (2 * kStages);
@@ -142,8 +154,8 @@ __global__ void __launch_bounds__(128, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // 1-D grid, N tiles fastest: the CTAs that share a row block of A run together and read it once from HBM
-    const int ntn = (N + kBN - 1) / kBN;
-    const int m0 = static_cast<int>(blockIdx.x / ntn) * kBM, n0 = static_cast<int>(blockIdx.x % ntn) * kBN;
+    const int ntn = (N + BN - 1) / BN;
+    const int m0 = static_cast<int>(blockIdx.x / ntn) * kBM, n0 = static_cast<int>(blockIdx.x % ntn) * BN;
     const int nkp = (K + kBK - 1) / kBK;  // K blocks of one operand pair
     const int nk = nkp * npairs;
 
@@ -157,7 +169,7 @@ __global__ void __launch_bounds__(128, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tslot), "r"(kTmemCols)
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tslot), "r"(BN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -167,55 +179,65 @@ __global__ void __launch_bounds__(128, 1)
     uint32_t tmem;
     asm volatile("ld.shared.u32 %0, [%1];" : "=r"(tmem) : "r"(tslot) : "memory");
 
+    // Roles are taken by whole warps: one lane issues, the other lanes of the
+    // warp wait at __syncwarp (not in a polling loop that would compete with
+    // the issuing lane for the warp's issue slots).
     int issued = 0;
-    if (warp == 0 && lane == 0) {
-        // ---- producer: TMA loads of the K blocks
-        for (int kb = 0; kb < nk; ++kb) {
-            const int s = kb % kStages, r = kb / kStages;
-            if (r >= 1 && !mbar_wait(empty_bar(s), (r - 1) & 1)) {
-                atomicExch(err, 1);
-                break;
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- producer: TMA loads of the K blocks
+            for (int kb = 0; kb < nk; ++kb) {
+                const int s = kb % kStages, r = kb / kStages;
+                if (r >= 1 && !mbar_wait(empty_bar(s), (r - 1) & 1)) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                const uint32_t a = base + s * kStageBytes, b = a + Cfg::kABytes;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full_bar(s)),
+                             "r"(kStageBytes)
+                             : "memory");
+                const int p = kb / nkp, x = (kb - p * nkp) * kBK;
+                tma_load_2d(a, &maps.a[p], x, m0, full_bar(s));
+                tma_load_2d(b, &maps.b[p], x, n0, full_bar(s));
+                issued = kb + 1;
             }
-            const uint32_t a = base + s * kStageBytes, b = a + kTileBytes;
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full_bar(s)), "r"(kStageBytes)
-                         : "memory");
-            const int p = kb / nkp, x = (kb - p * nkp) * kBK;
-            tma_load_2d(a, &maps.a[p], x, m0, full_bar(s));
-            tma_load_2d(b, &maps.b[p], x, n0, full_bar(s));
-            issued = kb + 1;
         }
-    } else if (warp == 1 && lane == 0) {
-        // ---- MMA issue
-        int kb = 0;
-        for (; kb < nk; ++kb) {
-            const int s = kb % kStages, r = kb / kStages;
-            if (!mbar_wait(full_bar(s), r & 1)) {
-                atomicExch(err, 1);
-                break;
-            }
-            tc_fence_after();
-            const uint32_t a = base + s * kStageBytes, b = a + kTileBytes;
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issue
+            int kb = 0;
+            for (; kb < nk; ++kb) {
+                const int s = kb % kStages, r = kb / kStages;
+                if (!mbar_wait(full_bar(s), r & 1)) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t a = base + s * kStageBytes, b = a + Cfg::kABytes;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {  // 32 bytes of K per instruction (16 BF16 or 8 TF32)
-                const uint64_t da = sw128_desc(a + 32u * k), db = sw128_desc(b + 32u * k);
-                const uint32_t accumulate = (kb > 0 || k > 0) ? 1u : 0u;
-                if constexpr (TF32)
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                        "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
-                        : "memory");
-                else
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                        "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
-                        : "memory");
+                for (int k = 0; k < 4; ++k) {  // 32 bytes of K per instruction (16 BF16 or 8 TF32)
+                    const uint64_t da = sw128_desc(a + 32u * k), db = sw128_desc(b + 32u * k);
+                    const uint32_t accumulate = (kb > 0 || k > 0) ? 1u : 0u;
+                    if constexpr (TF32)
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                            "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+                            : "memory");
+                    else
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                            "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+                            : "memory");
+                }
+                tc_commit(empty_bar(s));  // the stage is free once these MMAs have read it
             }
-            tc_commit(empty_bar(s));  // the stage is free once these MMAs have read it
+            asm volatile("st.shared.u32 [%0], %1;" ::"r"(cslot), "r"(kb) : "memory");
+            tc_commit(done_bar);  // every MMA issued above has completed
         }
-        asm volatile("st.shared.u32 [%0], %1;" ::"r"(cslot), "r"(kb) : "memory");
-        tc_commit(done_bar);  // every MMA issued above has completed
+        __syncwarp();
     }
 
     // ---- epilogue: the accumulator goes through shared memory (the ring is
@@ -230,10 +252,10 @@ __global__ void __launch_bounds__(128, 1)
     }
     tc_fence_after();
     __syncthreads();
-    float* stile = reinterpret_cast<float*>(smem_raw + (base - raw));  // [128][kBN + 1]
-    constexpr int kLd = kBN + 1;
+    float* stile = reinterpret_cast<float*>(smem_raw + (base - raw));  // [128][BN + 1]
+    constexpr int kLd = BN + 1;
     const int trow = warp * 32 + lane;
-    for (int c0 = 0; c0 < kBN; c0 += 16) {
+    for (int c0 = 0; c0 < BN; c0 += 16) {
         uint32_t v[16];
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
@@ -246,26 +268,29 @@ __global__ void __launch_bounds__(128, 1)
         for (int jj = 0; jj < 16; ++jj) stile[trow * kLd + c0 + jj] = __uint_as_float(v[jj]);
     }
     __syncthreads();
-    const int col = n0 + static_cast<int>(threadIdx.x);  // kBN == blockDim.x
-    if (done && col < N) {
-        const float bias = (o.kind == kTcEpiBiasGelu || o.kind == kTcEpiBias) ? o.bias[col] : 0.0f;
-        for (int rr = 0; rr < kBM; ++rr) {
-            const int row = m0 + rr;
-            if (row >= M) break;
-            const float val = stile[rr * kLd + threadIdx.x];
-            const long long off = static_cast<long long>(row) * o.ldo + col;
-            if (o.kind == kTcEpiBiasGelu) {
-                const float z = val + bias;
-                o.outf[off] = z;
-                static_cast<__nv_bfloat16*>(o.outh)[off] = __float2bfloat16(gelu_f(z));
-            } else if (o.kind == kTcEpiBias) {
-                o.outf[off] = val + bias;
-            } else if (o.kind == kTcEpiStore) {
-                o.outf[off] = val;
-            } else {
-                const float g = val * gelu_grad_f(o.aux[off]);
-                static_cast<__nv_bfloat16*>(o.outh)[off] = __float2bfloat16(g);
-                if (o.outf) o.outf[off] = g;
+    if (done) {
+        for (int cc = static_cast<int>(threadIdx.x); cc < BN; cc += 128) {
+            const int col = n0 + cc;
+            if (col >= N) break;
+            const float bias = (o.kind == kTcEpiBiasGelu || o.kind == kTcEpiBias) ? o.bias[col] : 0.0f;
+            for (int rr = 0; rr < kBM; ++rr) {
+                const int row = m0 + rr;
+                if (row >= M) break;
+                const float val = stile[rr * kLd + cc];
+                const long long off = static_cast<long long>(row) * o.ldo + col;
+                if (o.kind == kTcEpiBiasGelu) {
+                    const float z = val + bias;
+                    o.outf[off] = z;
+                    static_cast<__nv_bfloat16*>(o.outh)[off] = __float2bfloat16(gelu_f(z));
+                } else if (o.kind == kTcEpiBias) {
+                    o.outf[off] = val + bias;
+                } else if (o.kind == kTcEpiStore) {
+                    o.outf[off] = val;
+                } else {
+                    const float g = val * gelu_grad_f(o.aux[off]);
+                    static_cast<__nv_bfloat16*>(o.outh)[off] = __float2bfloat16(g);
+                    if (o.outf) o.outf[off] = g;
+                }
             }
         }
     }
@@ -273,7 +298,7 @@ __global__ void __launch_bounds__(128, 1)
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
     }
 }
 
@@ -308,23 +333,23 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 }
 
 // Tensor map of a row-major matrix [rows x cols] (leading dimension ld) of
-// BF16 or FP32 (read as TF32) elements, boxes of 128 rows x 128 bytes in the
-// 128-byte swizzled layout.
-bool make_map(CUtensorMap* map, const void* ptr, int rows, int cols, int ld, bool fp32)
+// BF16 or FP32 (read as TF32) elements, boxes of box_rows rows x 128 bytes in
+// the 128-byte swizzled layout.
+bool make_map(CUtensorMap* map, const void* ptr, int rows, int cols, int ld, bool fp32, int box_rows)
 {
     auto fn = encode_fn();
     if (!fn) return false;
     const int esize = fp32 ? 4 : 2;
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * esize};
-    const cuuint32_t box[2] = {static_cast<cuuint32_t>(128 / esize), static_cast<cuuint32_t>(kBM)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kRowBytes / esize), static_cast<cuuint32_t>(box_rows)};
     const cuuint32_t estr[2] = {1, 1};
     return fn(map, fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr),
               dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <bool TF32>
+template <bool TF32, int BN>
 bool configure()
 {
     static bool configured[64] = {};
@@ -332,12 +357,18 @@ bool configure()
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return false;
     if (!configured[dev]) {
-        if (cudaFuncSetAttribute(tc_gemm_kernel<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kSmemBytes)) != cudaSuccess)
+        if (cudaFuncSetAttribute(tc_gemm_kernel<TF32, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(TileCfg<BN>::kSmem)) != cudaSuccess)
             return false;
         configured[dev] = true;
     }
     return true;
+}
+
+template <bool TF32>
+bool configure_all()
+{
+    return configure<TF32, 128>() && configure<TF32, 256>();
 }
 
 bool eligible(const void* A, int lda, const void* B, int ldb, int esize)
@@ -351,7 +382,7 @@ bool eligible(const void* A, int lda, const void* B, int ldb, int esize)
 
 bool tc_gemm_eligible(const void* A, int lda, const void* B, int ldb) { return eligible(A, lda, B, ldb, 2); }
 
-bool tc_gemm_ready(bool tf32) { return encode_fn() != nullptr && (tf32 ? configure<true>() : configure<false>()); }
+bool tc_gemm_ready(bool tf32) { return encode_fn() != nullptr && (tf32 ? configure_all<true>() : configure_all<false>()); }
 
 bool tc_gemm(int M, int N, int K, const void* A, int lda, const void* B, int ldb, const TcGemmOut& o, int* err,
              cudaStream_t s)
@@ -366,19 +397,24 @@ bool tc_gemm_sum(int M, int N, int K, int npairs, const TcPair* pairs, bool tf32
     if (M <= 0 || N <= 0 || K <= 0 || npairs < 1 || npairs > 3) return false;
     for (int p = 0; p < npairs; ++p)
         if (!eligible(pairs[p].A, pairs[p].lda, pairs[p].B, pairs[p].ldb, tf32 ? 4 : 2)) return false;
-    if (!(tf32 ? configure<true>() : configure<false>())) return false;
+    if (!(tf32 ? configure_all<true>() : configure_all<false>())) return false;
+    const int bn = N >= 256 ? 256 : 128;  // wide tiles halve the re-reads of A
     TcMaps maps;
     for (int p = 0; p < npairs; ++p)
-        if (!make_map(&maps.a[p], pairs[p].A, M, K, pairs[p].lda, tf32) ||
-            !make_map(&maps.b[p], pairs[p].B, N, K, pairs[p].ldb, tf32))
+        if (!make_map(&maps.a[p], pairs[p].A, M, K, pairs[p].lda, tf32, kBM) ||
+            !make_map(&maps.b[p], pairs[p].B, N, K, pairs[p].ldb, tf32, bn))
             return false;
-    const long long tiles = static_cast<long long>((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM);
+    const long long tiles = static_cast<long long>((N + bn - 1) / bn) * ((M + kBM - 1) / kBM);
     if (tiles > 0x7fffffffll) return false;
     const dim3 grid(static_cast<unsigned>(tiles));
-    if (tf32)
-        tc_gemm_kernel<true><<<grid, 128, kSmemBytes, s>>>(maps, M, N, K, npairs, o, err);
+    if (tf32 && bn == 256)
+        tc_gemm_kernel<true, 256><<<grid, 128, TileCfg<256>::kSmem, s>>>(maps, M, N, K, npairs, o, err);
+    else if (tf32)
+        tc_gemm_kernel<true, 128><<<grid, 128, TileCfg<128>::kSmem, s>>>(maps, M, N, K, npairs, o, err);
+    else if (bn == 256)
+        tc_gemm_kernel<false, 256><<<grid, 128, TileCfg<256>::kSmem, s>>>(maps, M, N, K, npairs, o, err);
     else
-        tc_gemm_kernel<false><<<grid, 128, kSmemBytes, s>>>(maps, M, N, K, npairs, o, err);
+        tc_gemm_kernel<false, 128><<<grid, 128, TileCfg<128>::kSmem, s>>>(maps, M, N, K, npairs, o, err);
     return true;
 }
 

@@ -116,7 +116,9 @@ typedef struct hx_problem {
 /* hx_problem.flags: evaluate the Hamiltonian commutator -i[H, u_n] of every
  * ADO as matrix products on the tensor cores (tcgen05, TF32 operands in a
  * 3-term split product, FP32 accumulation), for a general dense Hermitian H
- * (h_csr with any number of entries per row, or h_diag / h_flip).  Needs
+ * (h_csr with any number of entries per row, or h_diag / h_flip).  The real
+ * diagonal of H stays in the exact elementwise term, and ADO 0 (rho_0) takes
+ * its product in FP64.  Needs
  * HX_PRECISION_MIXED, HX_FLAG_FULL_STATE, diagonal coupling operators and
  * 128 <= dim <= 1024; the states must be Hermitian (hx_ctx_write_state
  * checks).  No counterpart in the reference, whose H is diagonal
@@ -144,7 +146,7 @@ typedef struct hx_info {
 #define HX_PATH_FLIP 3u     /* comm_kernel + combine_kernel: couplings with spin flips */
 #define HX_PATH_CSR 4u      /* csr_comm_kernel + csr_combine_kernel: general sparse operators */
 #define HX_PATH_SMALL 5u    /* small_kernel: d <= 16 with sigma_z couplings (batched neighbour gathers) */
-#define HX_PATH_DENSE 6u    /* HX_FLAG_DENSE_H: tf32_split_kernel + tc_gemm_kernel (Y = X H) + band kernels */
+#define HX_PATH_DENSE 6u    /* HX_FLAG_DENSE_H: tf32_split_kernel + tc_gemm_kernel + zgemm_kernel + band kernels */
 
 /* Profiling counters (replaces src/library/backend_profiling.cpp:9-137). */
 typedef struct hx_counters {
@@ -272,6 +274,15 @@ int hx_ctx_state_device_ptr(hx_ctx* ctx, void** ptr);
  * host buffer (hierarchy_size * d * d complex).  Test hook for parity of the
  * fused kernel against the reference RHS (getdRhoSparse, src/liouville.cu:749-869). */
 int hx_ctx_rhs(hx_ctx* ctx, double* out, uint64_t n);
+
+/* Enqueue `count` evaluations of the tensor-core product of an
+ * HX_FLAG_DENSE_H context on its stream, on the current state and without
+ * changing it: parts = 1 the TF32 split of the state, 2 the GEMM
+ * Y = X H_off (on the split of the last evaluation), 3 both.  These are the
+ * first two kernels of every stage; the entry exists to time and profile them
+ * alone.  HX_ERR_UNSUPPORTED_EXECUTION for other contexts.  No counterpart in
+ * the reference. */
+int hx_ctx_dense_product(hx_ctx* ctx, uint32_t count, uint32_t parts);
 
 /* Device check that the state holds only finite values; returns
  * HX_ERR_NON_FINITE otherwise. */

@@ -36,11 +36,11 @@ def test_dense_rhs_matches_oracle(n):
     o.close()
     with capi.Context(p, precision="mixed", dense_h=True) as ctx:
         assert ctx.stage_path == "dense"
-        assert ctx.get_info().kernels_per_step == 4 * 5  # split, GEMM, up-term, band, ADO 0
+        assert ctx.get_info().kernels_per_step == 4 * 6  # split, GEMM, FP64 product of ADO 0, up-term, band, ADO 0
         ctx.set_state(x)
         r = ctx.rhs()
     scale = np.max(np.abs(ref))
-    assert np.max(np.abs(r[0] - ref[0])) <= 2e-6 * scale
+    assert np.max(np.abs(r[0] - ref[0])) <= 1e-6 * scale  # ADO 0 takes its product in FP64
     assert np.max(np.abs(r - ref)) <= 1e-5 * scale
     # the RHS of a Hermitian hierarchy is Hermitian, and the commutator part is traceless
     assert np.max(np.abs(r - np.conj(np.transpose(r, (0, 2, 1))))) <= 1e-5 * scale
