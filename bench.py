@@ -869,7 +869,7 @@ def run_dense(args, cfg: dict) -> None:
     """Dense H on the tensor cores (HX_FLAG_DENSE_H) against the plain FP64
     propagator for the same H (the CSR path, the only FP64 path for a dense
     H) on the same GPU.  The roofline is the tensor one: the GEMM kernel alone
-    (hx_ctx_dense_product, parts = 2) timed with CUDA events, algorithmic FLOPs
+    (hx_ctx_dense_product) timed with CUDA events, algorithmic FLOPs
     8 H d^3 per launch (the complex product X H_off of every ADO) and executed
     FLOPs 3x that (the TF32 split)."""
     import torch
@@ -907,11 +907,10 @@ def run_dense(args, cfg: dict) -> None:
     clk = clocks.stop()
     launches = int(ctx.counters().kernel_launches - c0.kernel_launches)
     info = ctx.get_info()
-    # the GEMM alone, and the split alone, on the current state
+    # the GEMM alone (split of X in shared memory) on the current state
     reps = 20
-    ctx.dense_product(2, 3)
-    gemm_ms = events_ms(lambda: ctx.dense_product(reps, 2)) / reps
-    split_ms = events_ms(lambda: ctx.dense_product(reps, 1)) / reps
+    ctx.dense_product(2)
+    gemm_ms = events_ms(lambda: ctx.dense_product(reps)) / reps
     ctx.close()
     value = H * args.steps / (ms / 1000.0)
 
@@ -919,11 +918,13 @@ def run_dense(args, cfg: dict) -> None:
     torch.backends.cuda.matmul.allow_tf32 = True
     a = torch.randn(H * d, 2 * d, device="cuda")
     b = torch.randn(2 * d, 2 * d, device="cuda")
+    c = torch.empty(H * d, 2 * d, device="cuda")
+    torch.cuda.synchronize()
     with torch.cuda.stream(stream):
         for _ in range(3):
-            a @ b
-        cublas_ms = events_ms(lambda: [a @ b for _ in range(reps)]) / reps
-    del a, b
+            torch.matmul(a, b, out=c)
+        cublas_ms = events_ms(lambda: [torch.matmul(a, b, out=c) for _ in range(reps)]) / reps
+    del a, b, c
 
     # plain FP64 propagator for the same dense H (CSR path) and the error against it
     c64 = capi.Context(p)
@@ -995,13 +996,12 @@ def run_dense(args, cfg: dict) -> None:
         "error_vs_fp64": {"trace_distance_max": max(td), "trace_distance_final": td[-1],
                           "energy_abs_max": max(en_err), "trace_abs_max": max(tr_err), "steps": n_err, "every": 10},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": tpeak, "unit": "TFLOP/s",
-                     "frac": achieved / tpeak, "traffic": profiled_traffic(args.config, "tc_gemm_kernel"),
-                     "peak_source": tpeak_src, "kernel": "tc_gemm_kernel<tf32, 256>",
+                     "frac": achieved / tpeak, "traffic": profiled_traffic(args.config, "tc_split_gemm_kernel"),
+                     "peak_source": tpeak_src, "kernel": "tc_split_gemm_kernel",
                      "algorithmic_flops_per_launch": alg, "executed_flops_per_launch": 3 * alg,
                      "executed_tflops": 3 * achieved, "launch_ms": gemm_ms,
                      "cublas_tf32_one_product_ms": cublas_ms,
-                     "cublas_tf32_tflops": alg / (cublas_ms / 1000.0) / 1e12,
-                     "split_kernel_ms": split_ms},
+                     "cublas_tf32_tflops": alg / (cublas_ms / 1000.0) / 1e12},
         "e2e": {"value": H * args.steps / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": H * d * d * 16 / args.steps,
                 "d2h_bytes_per_step": d * d * 16 + 24,
                 "path": "hx_ctx_write_state + hx_ctx_step_trace (rho0, <H> per step) + hx_ctx_read_rho0"},

@@ -148,7 +148,7 @@ def lib():
             L.hx_ctx_read_rho0.argtypes = [vp, vp, u64]
             L.hx_ctx_observables.argtypes = [vp, dp, dp, dp]
             L.hx_ctx_read_state.argtypes = [vp, vp, u64]
-            L.hx_ctx_dense_product.argtypes = [vp, u32, u32]
+            L.hx_ctx_dense_product.argtypes = [vp, u32]
             L.hx_ctx_write_state.argtypes = [vp, vp, u64]
             L.hx_ctx_state_device_ptr.argtypes = [vp, C.POINTER(vp)]
             L.hx_ctx_rhs.argtypes = [vp, vp, u64]
@@ -418,9 +418,9 @@ class Context:
         assert s.size == self.size * self.dim * self.dim
         _check(lib().hx_ctx_write_state(self._h, _p(s), 2 * s.size))
 
-    def dense_product(self, count: int = 1, parts: int = 3) -> None:
-        """Enqueue ``count`` tensor-core products of a ``dense_h`` context (parts: 1 split, 2 GEMM, 3 both)."""
-        _check(lib().hx_ctx_dense_product(self._h, C.c_uint32(count), C.c_uint32(parts)))
+    def dense_product(self, count: int = 1) -> None:
+        """Enqueue ``count`` tensor-core products Y = X H_off of a ``dense_h`` context (timing hook)."""
+        _check(lib().hx_ctx_dense_product(self._h, C.c_uint32(count)))
 
     def rhs(self) -> np.ndarray:
         out = np.zeros((self.size, self.dim, self.dim), np.complex128)

@@ -57,8 +57,8 @@ void release(hx_ctx* c)
                     c->ent_wc, c->ent_wa, c->order_perm, c->ado_keep, c->up_slot, c->up_ado, c->up_cnt,
                     c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf, c->rho32, c->ua32, c->ub32,
                     c->U32, c->diag32, c->vdiag32, c->hflip32, c->diag_herm, c->vbit, c->csr_ptr, c->csr_col,
-                    c->csr_val, c->pack_scale, c->pack_bad, c->dense_hr, c->dense_hr_lo, c->dense_xhi,
-                    c->dense_xlo, c->dense_y, c->dense_h64, c->dense_z0};
+                    c->csr_val, c->pack_scale, c->pack_bad, c->dense_hr, c->dense_hr_lo, c->dense_y,
+                    c->dense_h64, c->dense_z0};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -232,23 +232,16 @@ int buffer_id(const hx_ctx* c, const double2* p) { return p == c->rho ? 0 : (p =
 // apply exactly) for every ADO of the complex64 stage input u32, as the real
 // product [H d x 2d] x [2d x 2d] (interleaved complex rows of X times the
 // real form of H_off) in 3-term TF32 split form, X_hi H_hi + X_hi H_lo +
-// X_lo H_hi, FP32 accumulation.  Returns kernels launched.
-int launch_dense_product(hx_ctx* c, const float2* u32, unsigned parts = 3)
+// X_lo H_hi with FP32 accumulation; the split of X happens in shared memory
+// inside the GEMM (tc_split_gemm).  Returns kernels launched.
+int launch_dense_product(hx_ctx* c, const float2* u32)
 {
-    const long long n = 2ll * c->H * static_cast<long long>(c->slab);
-    if (parts & 1u)
-        hx::launch_tf32_split(reinterpret_cast<const float*>(u32), c->dense_xhi, c->dense_xlo, n, c->stream);
-    if (!(parts & 2u)) return 1;
     const int d2 = 2 * c->d;
-    const float *xh = c->dense_xhi, *xl = c->dense_xlo;
-    const hx::TcPair pairs[3] = {{xh, d2, c->dense_hr, d2}, {xh, d2, c->dense_hr_lo, d2}, {xl, d2, c->dense_hr, d2}};
-    hx::TcGemmOut o{};
-    o.kind = hx::kTcEpiStore;
-    o.outf = reinterpret_cast<float*>(c->dense_y);
-    o.ldo = d2;
-    if (!hx::tc_gemm_sum(static_cast<int>(c->H * c->d), d2, d2, 3, pairs, true, o, c->error_flag, c->stream))
+    if (!hx::tc_split_gemm(static_cast<int>(c->H * c->d), d2, d2, reinterpret_cast<const float*>(u32), d2,
+                           c->dense_hr, c->dense_hr_lo, d2, reinterpret_cast<float*>(c->dense_y), d2, c->error_flag,
+                           c->stream))
         c->launch_failed = true;
-    return (parts & 1u) ? 2 : 1;
+    return 1;
 }
 
 // One stage of the band kernels (hx_large.cu): the up-term kernel of tier
@@ -953,7 +946,6 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
             (rc = dev_alloc(c, &c->dense_z0, h64.size())) ||
             (rc = dev_alloc(c, &c->dense_hr, hi.size())) || (rc = dev_alloc(c, &c->dense_hr_lo, lo.size())) ||
             (rc = upload(c, c->dense_hr, hi)) || (rc = upload(c, c->dense_hr_lo, lo)) ||
-            (rc = dev_alloc(c, &c->dense_xhi, 2 * nstate)) || (rc = dev_alloc(c, &c->dense_xlo, 2 * nstate)) ||
             (rc = dev_alloc(c, &c->dense_y, nstate)) || (rc = dev_alloc(c, &c->csr_ptr, dense_h.ptr.size())) ||
             (rc = dev_alloc(c, &c->csr_col, std::max<size_t>(1, dense_h.col.size()))) ||
             (rc = dev_alloc(c, &c->csr_val, std::max<size_t>(1, dense_h.val.size()))) ||
@@ -1122,7 +1114,7 @@ int hx_ctx_info(const hx_ctx* c, hx_info* info)
     info->steps_done = c->steps_done;
     info->time = static_cast<double>(c->steps_done) * c->dt;
     int per_stage = (c->use_flip || c->use_csr || (c->use_fused && c->up_slots > 0)) ? 2 : 1;
-    if (c->use_large) per_stage = 1 + (c->up_slots > 0 ? 1 : 0) + (c->mixed ? 1 : 0) + (c->dense ? 3 : 0);
+    if (c->use_large) per_stage = 1 + (c->up_slots > 0 ? 1 : 0) + (c->mixed ? 1 : 0) + (c->dense ? 2 : 0);
     info->kernels_per_step = static_cast<uint32_t>(c->order) * per_stage;
     info->stage_path = c->dense     ? HX_PATH_DENSE
                        : c->use_csr ? HX_PATH_CSR
@@ -1475,12 +1467,11 @@ int hx_ctx_state_device_ptr(hx_ctx* c, void** ptr)
     return HX_OK;
 }
 
-int hx_ctx_dense_product(hx_ctx* c, uint32_t count, uint32_t parts)
+int hx_ctx_dense_product(hx_ctx* c, uint32_t count)
 {
     if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
     if (!c->dense) return fail(HX_ERR_UNSUPPORTED_EXECUTION, "not an HX_FLAG_DENSE_H context");
-    if (parts < 1 || parts > 3) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "parts must be 1, 2 or 3");
-    for (uint32_t i = 0; i < count; ++i) c->counters.kernel_launches += launch_dense_product(c, c->rho32, parts);
+    for (uint32_t i = 0; i < count; ++i) c->counters.kernel_launches += launch_dense_product(c, c->rho32);
     const int rc = check_launch("dense product");
     if (rc != HX_OK) return rc;
     if (c->launch_failed) {

@@ -179,8 +179,10 @@ bool tc_gemm_sum(int M, int N, int K, int npairs, const TcPair* pairs, bool tf32
                  cudaStream_t s);
 // The driver entry point and kernel attributes the tensor-core GEMM needs are available.
 bool tc_gemm_ready(bool tf32);
-// TF32 split of n floats (16-byte aligned): hi = tf32(x), lo = tf32(x - hi), both exact TF32 values
-void launch_tf32_split(const float* x, float* hi, float* lo, long long n, cudaStream_t s);
+// C [M x N] = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T with the TF32 split of the FP32 operand A done in
+// shared memory (B_hi, B_lo exact TF32 values, N <= 256 per tile column); FP32 result, row length ldo.
+bool tc_split_gemm(int M, int N, int K, const float* A, int lda, const float* Bhi, const float* Blo, int ldb,
+                   float* out, int ldo, int* err, cudaStream_t s);
 void launch_transpose_bf16(const void* in, int rows, int cols, int ld_in, void* out, int ld_out, cudaStream_t s);
 // d <= 16, full slabs, sigma_z couplings, every up term in the entry lists: batched gathers (hx_small.cu)
 size_t small_smem(int logd, int M);
@@ -430,8 +432,6 @@ struct hx_ctx {
     bool dense = false;
     float* dense_hr = nullptr;    // [2d][2d] real form of H_off, K-major: row 2c = (Re H_kc, -Im H_kc)_k,
     float* dense_hr_lo = nullptr; //   row 2c+1 = (Im H_kc, Re H_kc)_k; and its TF32 residual
-    float* dense_xhi = nullptr;   // [H][d][2d] TF32 split of the stage input
-    float* dense_xlo = nullptr;
     float2* dense_y = nullptr;    // [H][d][d] Y_n = X_n H_off (H without its diagonal)
     double2* dense_h64 = nullptr; // [d][d] H_off in FP64 (ADO 0's product)
     double2* dense_z0 = nullptr;  // [d][d] Z_0 = X_0 H_off in FP64

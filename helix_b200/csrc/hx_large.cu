@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(256, 2)
             R hr = 0, hi = 0;
 #pragma unroll
             for (int i = 0; i < LOGD; ++i) {
+                if (sH[i] == R(0)) continue;  // no field on this spin (every spin with a dense H): no gathers
                 constexpr long long one = 1;
                 const long long fb = static_cast<long long>(D) << i;  // row bit i of the element index
                 C rowp;

@@ -302,6 +302,213 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
+// FP32 value rounded to TF32 (10 mantissa bits, to nearest, ties away from zero).
+__device__ __forceinline__ float tf32_round(float v)
+{
+    return __uint_as_float((__float_as_uint(v) + 0x1000u) & 0xFFFFE000u);
+}
+
+// Split-product GEMM with the split of A done in shared memory:
+// C = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T, A [M x K] FP32, B_hi / B_lo
+// [256 x K] exact TF32 values, FP32 accumulation (the dense-H product).  Each
+// stage holds one K block of A (rounded in place to A_hi), of A_lo, of B_hi
+// and of B_lo (16 + 16 + 32 + 32 KB); two stages fill the 192 KB ring.
+//  * warp 0 lane 0: TMA loads of A, B_hi, B_lo;
+//  * warps 2-3: once a stage has landed, round A to A_hi in place and write
+//    A_lo beside it (an elementwise map at equal offsets, so the swizzled
+//    layout carries over), fence the writes to the tensor cores' proxy and
+//    arrive on the stage's conversion barrier;
+//  * warp 1 lane 0: twelve tcgen05.mma per stage (three products x four
+//    K steps of 8), then tcgen05.commit frees the stage;
+//  * the epilogue of tc_gemm_kernel (plain store).
+// A is read from HBM once and never written back in split form.
+constexpr int kSplitBN = 256, kSplitStages = 2;
+constexpr uint32_t kSplitA = kBM * kRowBytes, kSplitB = kSplitBN * kRowBytes;
+constexpr uint32_t kSplitStage = 2 * kSplitA + 2 * kSplitB;
+constexpr uint32_t kSplitRing = kSplitStages * kSplitStage;
+constexpr uint32_t kSplitSmem = kSplitRing + 1024 + 256;
+static_assert(kBM * (kSplitBN + 1) * 4 <= kSplitRing, "the epilogue tile reuses the ring");
+static_assert(kSplitSmem <= 227 * 1024, "shared memory per CTA");
+constexpr int kConvThreads = 64;
+
+__global__ void __launch_bounds__(128, 1)
+    tc_split_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_bh,
+                         const __grid_constant__ CUtensorMap map_bl, int M, int N, int K, float* out, int ldo,
+                         int* err)
+{
+    constexpr int kBK = 32;  // TF32 per 128-byte row
+    constexpr uint32_t kIdesc = idesc_of(2u, kSplitBN);
+    extern __shared__ unsigned char smem_raw[];
+    const uint32_t raw = saddr(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - raw);  // generic pointer to the ring
+    const uint32_t bars = base + kSplitRing;
+    auto full_bar = [&](int s) { return bars + 8u * s; };
+    auto conv_bar = [&](int s) { return bars + 8u * (kSplitStages + s); };
+    auto empty_bar = [&](int s) { return bars + 8u * (2 * kSplitStages + s); };
+    const uint32_t done_bar = bars + 8u * (3 * kSplitStages);
+    const uint32_t tslot = done_bar + 8u;
+    const uint32_t cslot = tslot + 4u;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntn = (N + kSplitBN - 1) / kSplitBN;
+    const int m0 = static_cast<int>(blockIdx.x / ntn) * kBM, n0 = static_cast<int>(blockIdx.x % ntn) * kSplitBN;
+    const int nk = (K + kBK - 1) / kBK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kSplitStages; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(conv_bar(s), kConvThreads);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(done_bar, 1);
+        asm volatile("st.shared.u32 [%0], %1;" ::"r"(cslot), "r"(0) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tslot),
+                     "r"(kSplitBN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    uint32_t tmem;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(tmem) : "r"(tslot) : "memory");
+
+    int issued = 0;
+    if (warp == 0) {
+        if (lane == 0) {
+            for (int kb = 0; kb < nk; ++kb) {
+                const int s = kb % kSplitStages, r = kb / kSplitStages;
+                if (r >= 1 && !mbar_wait(empty_bar(s), (r - 1) & 1)) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                const uint32_t a = base + s * kSplitStage;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full_bar(s)),
+                             "r"(kSplitA + 2 * kSplitB)
+                             : "memory");
+                const int x = kb * kBK;
+                tma_load_2d(a, &map_a, x, m0, full_bar(s));
+                tma_load_2d(a + 2 * kSplitA, &map_bh, x, n0, full_bar(s));
+                tma_load_2d(a + 2 * kSplitA + kSplitB, &map_bl, x, n0, full_bar(s));
+                issued = kb + 1;
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int kb = 0;
+            for (; kb < nk; ++kb) {
+                const int s = kb % kSplitStages, r = kb / kSplitStages;
+                if (!mbar_wait(conv_bar(s), r & 1)) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t ah = base + s * kSplitStage, al = ah + kSplitA, bh = ah + 2 * kSplitA,
+                               bl = bh + kSplitB;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const uint64_t dah = sw128_desc(ah + 32u * k), dal = sw128_desc(al + 32u * k),
+                                   dbh = sw128_desc(bh + 32u * k), dbl = sw128_desc(bl + 32u * k);
+                    const uint32_t first = (kb == 0 && k == 0) ? 0u : 1u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                        "l"(dal), "l"(dbh), "r"(kIdesc), "r"(first)
+                        : "memory");
+                    asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tmem), "l"(dah),
+                                 "l"(dbl), "r"(kIdesc)
+                                 : "memory");
+                    asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tmem), "l"(dah),
+                                 "l"(dbh), "r"(kIdesc)
+                                 : "memory");
+                }
+                tc_commit(empty_bar(s));
+            }
+            asm volatile("st.shared.u32 [%0], %1;" ::"r"(cslot), "r"(kb) : "memory");
+            tc_commit(done_bar);
+        }
+        __syncwarp();
+    } else {
+        // converters: A -> A_hi in place, A_lo beside it
+        const int t = threadIdx.x - 64;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kSplitStages, r = kb / kSplitStages;
+            if (!mbar_wait(full_bar(s), r & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+            float4* ah = reinterpret_cast<float4*>(gbase + s * kSplitStage);
+            float4* al = reinterpret_cast<float4*>(gbase + s * kSplitStage + kSplitA);
+#pragma unroll 4
+            for (int i = t; i < static_cast<int>(kSplitA / 16); i += kConvThreads) {
+                const float4 v = ah[i];
+                float4 h, l;
+                h.x = tf32_round(v.x);
+                h.y = tf32_round(v.y);
+                h.z = tf32_round(v.z);
+                h.w = tf32_round(v.w);
+                l.x = tf32_round(v.x - h.x);
+                l.y = tf32_round(v.y - h.y);
+                l.z = tf32_round(v.z - h.z);
+                l.w = tf32_round(v.w - h.w);
+                ah[i] = h;
+                al[i] = l;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(conv_bar(s)) : "memory");
+        }
+    }
+
+    const bool done = mbar_wait(done_bar, 0);
+    if (!done && threadIdx.x == 0) atomicExch(err, 1);
+    if (warp == 0 && lane == 0) {
+        int consumed;
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(consumed) : "r"(cslot) : "memory");
+        for (int kb = consumed; kb < issued; ++kb) mbar_wait(full_bar(kb % kSplitStages), (kb / kSplitStages) & 1);
+    }
+    tc_fence_after();
+    __syncthreads();
+    float* stile = reinterpret_cast<float*>(gbase);  // [128][kSplitBN + 1]
+    constexpr int kLd = kSplitBN + 1;
+    const int trow = warp * 32 + lane;
+    for (int c0 = 0; c0 < kSplitBN; c0 += 16) {
+        uint32_t v[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) stile[trow * kLd + c0 + jj] = __uint_as_float(v[jj]);
+    }
+    __syncthreads();
+    if (done) {
+        for (int cc = static_cast<int>(threadIdx.x); cc < kSplitBN; cc += 128) {
+            const int col = n0 + cc;
+            if (col >= N) break;
+            for (int rr = 0; rr < kBM; ++rr) {
+                const int row = m0 + rr;
+                if (row >= M) break;
+                out[static_cast<long long>(row) * ldo + col] = stile[rr * kLd + cc];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kSplitBN)
+                     : "memory");
+    }
+}
+
 // Row-major BF16 transpose: out[c][r] = in[r][c] for rows x cols.
 __global__ void transpose_bf16_kernel(const __nv_bfloat16* __restrict__ in, int rows, int cols, int ld_in,
                                       __nv_bfloat16* __restrict__ out, int ld_out)
@@ -418,48 +625,29 @@ bool tc_gemm_sum(int M, int N, int K, int npairs, const TcPair* pairs, bool tf32
     return true;
 }
 
-// TF32 split of FP32 values: hi = x rounded to TF32 (10 mantissa bits, to
-// nearest, ties away from zero), lo = (x - hi) rounded the same way; both are
-// exact TF32 values, so the products do not depend on how the tensor cores
-// treat the low mantissa bits of an FP32 operand.  |x - hi - lo| <= 2^-22 |x|,
-// and A B ~ A_hi B_hi + A_hi B_lo + A_lo B_hi leaves out terms of that order.
-__device__ __forceinline__ float tf32_round(float v)
+bool tc_split_gemm(int M, int N, int K, const float* A, int lda, const float* Bhi, const float* Blo, int ldb,
+                   float* out, int ldo, int* err, cudaStream_t s)
 {
-    return __uint_as_float((__float_as_uint(v) + 0x1000u) & 0xFFFFE000u);
-}
-
-__global__ void tf32_split_kernel(const float* __restrict__ x, float* __restrict__ hi, float* __restrict__ lo,
-                                  long long n)
-{
-    const long long n4 = n >> 2;
-    const float4* x4 = reinterpret_cast<const float4*>(x);
-    float4* h4 = reinterpret_cast<float4*>(hi);
-    float4* l4 = reinterpret_cast<float4*>(lo);
-    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n4; i += stride) {
-        const float4 v = __ldcs(x4 + i);
-        float4 h, l;
-        h.x = tf32_round(v.x);
-        h.y = tf32_round(v.y);
-        h.z = tf32_round(v.z);
-        h.w = tf32_round(v.w);
-        l.x = tf32_round(v.x - h.x);
-        l.y = tf32_round(v.y - h.y);
-        l.z = tf32_round(v.z - h.z);
-        l.w = tf32_round(v.w - h.w);
-        h4[i] = h;
-        l4[i] = l;
+    if (M <= 0 || N <= 0 || K <= 0) return false;
+    if (!eligible(A, lda, Bhi, ldb, 4) || !eligible(A, lda, Blo, ldb, 4)) return false;
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return false;
+    if (!configured[dev]) {
+        if (cudaFuncSetAttribute(tc_split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kSplitSmem)) != cudaSuccess)
+            return false;
+        configured[dev] = true;
     }
-    for (long long i = 4 * n4 + blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n; i += stride) {
-        const float h = tf32_round(x[i]);
-        hi[i] = h;
-        lo[i] = tf32_round(x[i] - h);
-    }
-}
-
-void launch_tf32_split(const float* x, float* hi, float* lo, long long n, cudaStream_t s)
-{
-    tf32_split_kernel<<<148 * 8, 256, 0, s>>>(x, hi, lo, n);
+    CUtensorMap ma, mbh, mbl;
+    if (!make_map(&ma, A, M, K, lda, true, kBM) || !make_map(&mbh, Bhi, N, K, ldb, true, kSplitBN) ||
+        !make_map(&mbl, Blo, N, K, ldb, true, kSplitBN))
+        return false;
+    const long long tiles = static_cast<long long>((N + kSplitBN - 1) / kSplitBN) * ((M + kBM - 1) / kBM);
+    if (tiles > 0x7fffffffll) return false;
+    tc_split_gemm_kernel<<<static_cast<unsigned>(tiles), 128, kSplitSmem, s>>>(ma, mbh, mbl, M, N, K, out, ldo, err);
+    return true;
 }
 
 void launch_transpose_bf16(const void* in, int rows, int cols, int ld_in, void* out, int ld_out, cudaStream_t s)

@@ -146,7 +146,7 @@ typedef struct hx_info {
 #define HX_PATH_FLIP 3u     /* comm_kernel + combine_kernel: couplings with spin flips */
 #define HX_PATH_CSR 4u      /* csr_comm_kernel + csr_combine_kernel: general sparse operators */
 #define HX_PATH_SMALL 5u    /* small_kernel: d <= 16 with sigma_z couplings (batched neighbour gathers) */
-#define HX_PATH_DENSE 6u    /* HX_FLAG_DENSE_H: tf32_split_kernel + tc_gemm_kernel + zgemm_kernel + band kernels */
+#define HX_PATH_DENSE 6u    /* HX_FLAG_DENSE_H: tc_split_gemm_kernel + zgemm_kernel + band kernels */
 
 /* Profiling counters (replaces src/library/backend_profiling.cpp:9-137). */
 typedef struct hx_counters {
@@ -275,14 +275,13 @@ int hx_ctx_state_device_ptr(hx_ctx* ctx, void** ptr);
  * fused kernel against the reference RHS (getdRhoSparse, src/liouville.cu:749-869). */
 int hx_ctx_rhs(hx_ctx* ctx, double* out, uint64_t n);
 
-/* Enqueue `count` evaluations of the tensor-core product of an
- * HX_FLAG_DENSE_H context on its stream, on the current state and without
- * changing it: parts = 1 the TF32 split of the state, 2 the GEMM
- * Y = X H_off (on the split of the last evaluation), 3 both.  These are the
- * first two kernels of every stage; the entry exists to time and profile them
- * alone.  HX_ERR_UNSUPPORTED_EXECUTION for other contexts.  No counterpart in
- * the reference. */
-int hx_ctx_dense_product(hx_ctx* ctx, uint32_t count, uint32_t parts);
+/* Enqueue `count` evaluations of the tensor-core product Y = X H_off of an
+ * HX_FLAG_DENSE_H context (tc_split_gemm_kernel, the first kernel of every
+ * stage) on its stream, on the current state and without changing it: the
+ * entry exists to time and profile the product alone.
+ * HX_ERR_UNSUPPORTED_EXECUTION for other contexts.  No counterpart in the
+ * reference. */
+int hx_ctx_dense_product(hx_ctx* ctx, uint32_t count);
 
 /* Device check that the state holds only finite values; returns
  * HX_ERR_NON_FINITE otherwise. */

@@ -36,7 +36,7 @@ def test_dense_rhs_matches_oracle(n):
     o.close()
     with capi.Context(p, precision="mixed", dense_h=True) as ctx:
         assert ctx.stage_path == "dense"
-        assert ctx.get_info().kernels_per_step == 4 * 6  # split, GEMM, FP64 product of ADO 0, up-term, band, ADO 0
+        assert ctx.get_info().kernels_per_step == 4 * 5  # GEMM, FP64 product of ADO 0, up-term, band, ADO 0
         ctx.set_state(x)
         r = ctx.rhs()
     scale = np.max(np.abs(ref))
