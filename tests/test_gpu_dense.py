@@ -81,6 +81,27 @@ def test_dense_matches_fp64_csr_path_at_c3_shape():
     assert np.all(np.isfinite(state))
 
 
+@pytest.mark.parametrize("n", [9, 10])
+def test_dense_matches_fp64_csr_path_at_d512_and_d1024(n):
+    """The wider shapes of every dense-path kernel: GEMM with 4 and 8 column
+    tiles (N = 2d), band strips of 8 and 4 rows, the FP64 product of rho_0 on
+    16 x 16 and 32 x 32 tile grids; 10 steps against the FP64 CSR path."""
+    p = S.dense_h_problem(n, seed=60 + n, depth=2, K=1, n_baths=2, dt=0.005)
+    steps = 10
+    with capi.Context(p) as c64:
+        assert c64.stage_path == "csr"
+        r64, e64 = c64.step_trace(steps)
+    with capi.Context(p, precision="mixed", dense_h=True) as cm:
+        assert cm.stage_path == "dense"
+        rm, em = cm.step_trace(steps)
+        e, tr = cm.observables()
+    td = [_trace_distance(rm[t], r64[t]) for t in range(steps)]
+    assert max(td) <= TD_TOL, max(td)
+    assert np.max(np.abs(em - e64)) <= 1e-6
+    assert abs(tr - 1.0) <= 1e-9
+    assert np.max(np.abs(r64[-1] - r64[0])) > 1e-4
+
+
 def test_dense_rejects_non_hermitian_states_and_unsupported_shapes():
     p = S.dense_h_problem(7, seed=1, depth=2, K=1, n_baths=2)
     with capi.Context(p, precision="mixed", dense_h=True) as ctx:
