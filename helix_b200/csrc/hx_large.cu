@@ -52,13 +52,19 @@ __device__ __forceinline__ C2<R> mk(R x, R y)
     return v;
 }
 
+// Threads of a full-slab band CTA: complex64 bands take twice the threads
+// (8 elements each instead of 16), so twice the warps per SM hide the
+// neighbour gathers' latency at the same shared memory per CTA.
+template <typename R> struct LargeThreads { static constexpr int T = 256; };
+template <> struct LargeThreads<float> { static constexpr int T = 512; };
+
 template <typename R, int LOGD>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(LargeThreads<R>::T, 2)
     large_kernel(LargeArgs<R> a, const C2<R>* __restrict__ u, const C2<R>* rho, C2<R>* out, double alpha_d,
                  int base_kind)
 {
     using C = C2<R>;
-    constexpr int D = 1 << LOGD, T = 256, BE = 4096, E = BE / T, CH = 4;
+    constexpr int D = 1 << LOGD, T = LargeThreads<R>::T, BE = 4096, E = BE / T, CH = 4;
     constexpr long long D2 = static_cast<long long>(D) * D;
     constexpr int NB = static_cast<int>(D2 / BE);  // bands per slab
     extern __shared__ __align__(128) unsigned char smem[];
@@ -619,7 +625,7 @@ bool launch_t(const LargeArgs<R>& a, const C2<R>* u, const C2<R>* rho, C2<R>* ou
     if (nb <= 0) return true;
     if (a.herm)
         herm_band_kernel<R, LOGD><<<static_cast<unsigned>(nb), BandThreads<R>::T, smem, s>>>(a, u, rho, out, alpha, base);
-    else large_kernel<R, LOGD><<<static_cast<unsigned>(nb), 256, smem, s>>>(a, u, rho, out, alpha, base);
+    else large_kernel<R, LOGD><<<static_cast<unsigned>(nb), LargeThreads<R>::T, smem, s>>>(a, u, rho, out, alpha, base);
     return true;
 }
 
