@@ -310,28 +310,37 @@ __device__ __forceinline__ float tf32_round(float v)
 
 // Split-product GEMM with the split of A done in shared memory:
 // C = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T, A [M x K] FP32, B_hi / B_lo
-// [256 x K] exact TF32 values, FP32 accumulation (the dense-H product).  Each
-// stage holds one K block of A (rounded in place to A_hi), of A_lo, of B_hi
-// and of B_lo (16 + 16 + 32 + 32 KB); two stages fill the 192 KB ring.
-//  * warp 0 lane 0: TMA loads of A, B_hi, B_lo;
+// [N x K] exact TF32 values, FP32 accumulation (the dense-H product).
+// Persistent: one CTA per SM walks the 128 x 256 tiles (N tiles fastest), with
+// two accumulators in tensor memory (2 x 256 columns) so that the epilogue of
+// one tile overlaps the MMAs of the next.  Each ring stage holds one K block
+// of A (rounded in place to A_hi), of A_lo, of B_hi and of B_lo
+// (16 + 16 + 32 + 32 KB); two stages fill 192 KB.
+//  * warp 0 lane 0: TMA loads of A, B_hi, B_lo for every K block of every tile;
 //  * warps 2-3: once a stage has landed, round A to A_hi in place and write
 //    A_lo beside it (an elementwise map at equal offsets, so the swizzled
 //    layout carries over), fence the writes to the tensor cores' proxy and
 //    arrive on the stage's conversion barrier;
-//  * warp 1 lane 0: twelve tcgen05.mma per stage (three products x four
-//    K steps of 8), then tcgen05.commit frees the stage;
-//  * the epilogue of tc_gemm_kernel (plain store).
-// A is read from HBM once and never written back in split form.
+//  * warp 1 lane 0: twelve tcgen05.mma per stage (three products x four K
+//    steps of 8; the small terms first), tcgen05.commit frees the stage, and
+//    after a tile's last K block a commit marks its accumulator full;
+//  * warps 4-7: each reads its 32 lanes (rows) of a full accumulator 32
+//    columns at a time, transposes them through 4 KB of shared memory and
+//    stores whole 128-byte row pieces, then frees the accumulator.
+// A is read from HBM once and never written back in split form.  Every wait
+// is bounded; a wait that runs out sets the error word and its role stops.
 constexpr int kSplitBN = 256, kSplitStages = 2;
 constexpr uint32_t kSplitA = kBM * kRowBytes, kSplitB = kSplitBN * kRowBytes;
 constexpr uint32_t kSplitStage = 2 * kSplitA + 2 * kSplitB;
 constexpr uint32_t kSplitRing = kSplitStages * kSplitStage;
-constexpr uint32_t kSplitSmem = kSplitRing + 1024 + 256;
-static_assert(kBM * (kSplitBN + 1) * 4 <= kSplitRing, "the epilogue tile reuses the ring");
+constexpr int kEpiWarps = 4;
+constexpr uint32_t kEpiBuf = 32 * 33 * 4;  // one epilogue warp's 32 x 32 block, padded rows
+constexpr uint32_t kSplitSmem = kSplitRing + kEpiWarps * kEpiBuf + 1024 + 256;
 static_assert(kSplitSmem <= 227 * 1024, "shared memory per CTA");
 constexpr int kConvThreads = 64;
+constexpr int kSplitThreads = 256;
 
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kSplitThreads, 1)
     tc_split_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_bh,
                          const __grid_constant__ CUtensorMap map_bl, int M, int N, int K, float* out, int ldo,
                          int* err)
@@ -342,18 +351,27 @@ __global__ void __launch_bounds__(128, 1)
     const uint32_t raw = saddr(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     unsigned char* gbase = smem_raw + (base - raw);  // generic pointer to the ring
-    const uint32_t bars = base + kSplitRing;
+    const uint32_t bars = base + kSplitRing + kEpiWarps * kEpiBuf;
     auto full_bar = [&](int s) { return bars + 8u * s; };
-    auto conv_bar = [&](int s) { return bars + 8u * (kSplitStages + s); };
-    auto empty_bar = [&](int s) { return bars + 8u * (2 * kSplitStages + s); };
-    const uint32_t done_bar = bars + 8u * (3 * kSplitStages);
-    const uint32_t tslot = done_bar + 8u;
-    const uint32_t cslot = tslot + 4u;
+    auto conv_bar = [&](int s) { return bars + 8u * (2 + s); };
+    auto empty_bar = [&](int s) { return bars + 8u * (4 + s); };
+    auto accf_bar = [&](int x) { return bars + 8u * (6 + x); };
+    auto acce_bar = [&](int x) { return bars + 8u * (8 + x); };
+    const uint32_t fin_bar = bars + 8u * 10;
+    const uint32_t tslot = bars + 8u * 11;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntn = (N + kSplitBN - 1) / kSplitBN;
-    const int m0 = static_cast<int>(blockIdx.x / ntn) * kBM, n0 = static_cast<int>(blockIdx.x % ntn) * kSplitBN;
+    const int tiles = ntn * ((M + kBM - 1) / kBM);
+    const int mine = tiles > static_cast<int>(blockIdx.x)
+                         ? (tiles - 1 - static_cast<int>(blockIdx.x)) / static_cast<int>(gridDim.x) + 1
+                         : 0;
     const int nk = (K + kBK - 1) / kBK;
+    auto tile_of = [&](int i, int& m0, int& n0) {
+        const int t = static_cast<int>(blockIdx.x) + i * static_cast<int>(gridDim.x);
+        m0 = (t / ntn) * kBM;
+        n0 = (t % ntn) * kSplitBN;
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kSplitStages; ++s) {
@@ -361,13 +379,16 @@ __global__ void __launch_bounds__(128, 1)
             mbar_init(conv_bar(s), kConvThreads);
             mbar_init(empty_bar(s), 1);
         }
-        mbar_init(done_bar, 1);
-        asm volatile("st.shared.u32 [%0], %1;" ::"r"(cslot), "r"(0) : "memory");
+        for (int x = 0; x < 2; ++x) {
+            mbar_init(accf_bar(x), 1);
+            mbar_init(acce_bar(x), kEpiWarps);
+        }
+        mbar_init(fin_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tslot),
-                     "r"(kSplitBN)
+                     "r"(2 * kSplitBN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -377,68 +398,93 @@ __global__ void __launch_bounds__(128, 1)
     uint32_t tmem;
     asm volatile("ld.shared.u32 %0, [%1];" : "=r"(tmem) : "r"(tslot) : "memory");
 
-    int issued = 0;
     if (warp == 0) {
         if (lane == 0) {
-            for (int kb = 0; kb < nk; ++kb) {
-                const int s = kb % kSplitStages, r = kb / kSplitStages;
-                if (r >= 1 && !mbar_wait(empty_bar(s), (r - 1) & 1)) {
-                    atomicExch(err, 1);
-                    break;
+            // ---- producer
+            long long g = 0;
+            bool ok = true;
+            for (int i = 0; i < mine && ok; ++i) {
+                int m0, n0;
+                tile_of(i, m0, n0);
+                for (int kb = 0; kb < nk; ++kb, ++g) {
+                    const int s = static_cast<int>(g & 1);
+                    const long long r = g >> 1;
+                    if (r >= 1 && !mbar_wait(empty_bar(s), static_cast<uint32_t>((r - 1) & 1))) {
+                        atomicExch(err, 1);
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t a = base + s * kSplitStage;
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full_bar(s)),
+                                 "r"(kSplitA + 2 * kSplitB)
+                                 : "memory");
+                    const int x = kb * kBK;
+                    tma_load_2d(a, &map_a, x, m0, full_bar(s));
+                    tma_load_2d(a + 2 * kSplitA, &map_bh, x, n0, full_bar(s));
+                    tma_load_2d(a + 2 * kSplitA + kSplitB, &map_bl, x, n0, full_bar(s));
                 }
-                const uint32_t a = base + s * kSplitStage;
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full_bar(s)),
-                             "r"(kSplitA + 2 * kSplitB)
-                             : "memory");
-                const int x = kb * kBK;
-                tma_load_2d(a, &map_a, x, m0, full_bar(s));
-                tma_load_2d(a + 2 * kSplitA, &map_bh, x, n0, full_bar(s));
-                tma_load_2d(a + 2 * kSplitA + kSplitB, &map_bl, x, n0, full_bar(s));
-                issued = kb + 1;
             }
+            // at most the last two issued copies can still be in flight: wait for them (bounded)
+            for (long long h = g > 2 ? g - 2 : 0; h < g; ++h)
+                mbar_wait(full_bar(static_cast<int>(h & 1)), static_cast<uint32_t>((h >> 1) & 1));
         }
         __syncwarp();
     } else if (warp == 1) {
         if (lane == 0) {
-            int kb = 0;
-            for (; kb < nk; ++kb) {
-                const int s = kb % kSplitStages, r = kb / kSplitStages;
-                if (!mbar_wait(conv_bar(s), r & 1)) {
+            // ---- MMA issue
+            long long g = 0;
+            bool ok = true;
+            for (int i = 0; i < mine && ok; ++i) {
+                const int x = i & 1;
+                if (i >= 2 && !mbar_wait(acce_bar(x), static_cast<uint32_t>(((i >> 1) - 1) & 1))) {
                     atomicExch(err, 1);
                     break;
                 }
                 tc_fence_after();
-                const uint32_t ah = base + s * kSplitStage, al = ah + kSplitA, bh = ah + 2 * kSplitA,
-                               bl = bh + kSplitB;
+                const uint32_t tacc = tmem + static_cast<uint32_t>(x * kSplitBN);
+                for (int kb = 0; kb < nk; ++kb, ++g) {
+                    const int s = static_cast<int>(g & 1);
+                    if (!mbar_wait(conv_bar(s), static_cast<uint32_t>((g >> 1) & 1))) {
+                        atomicExch(err, 1);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t ah = base + s * kSplitStage, al = ah + kSplitA, bh = ah + 2 * kSplitA,
+                                   bl = bh + kSplitB;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const uint64_t dah = sw128_desc(ah + 32u * k), dal = sw128_desc(al + 32u * k),
-                                   dbh = sw128_desc(bh + 32u * k), dbl = sw128_desc(bl + 32u * k);
-                    const uint32_t first = (kb == 0 && k == 0) ? 0u : 1u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                        "l"(dal), "l"(dbh), "r"(kIdesc), "r"(first)
-                        : "memory");
-                    asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tmem), "l"(dah),
-                                 "l"(dbl), "r"(kIdesc)
-                                 : "memory");
-                    asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tmem), "l"(dah),
-                                 "l"(dbh), "r"(kIdesc)
-                                 : "memory");
+                    for (int k = 0; k < 4; ++k) {
+                        const uint64_t dah = sw128_desc(ah + 32u * k), dal = sw128_desc(al + 32u * k),
+                                       dbh = sw128_desc(bh + 32u * k), dbl = sw128_desc(bl + 32u * k);
+                        const uint32_t acc = (kb == 0 && k == 0) ? 0u : 1u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tacc),
+                            "l"(dal), "l"(dbh), "r"(kIdesc), "r"(acc)
+                            : "memory");
+                        asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tacc),
+                                     "l"(dah), "l"(dbl), "r"(kIdesc)
+                                     : "memory");
+                        asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tacc),
+                                     "l"(dah), "l"(dbh), "r"(kIdesc)
+                                     : "memory");
+                    }
+                    tc_commit(empty_bar(s));
                 }
-                tc_commit(empty_bar(s));
+                if (ok) tc_commit(accf_bar(x));
             }
-            asm volatile("st.shared.u32 [%0], %1;" ::"r"(cslot), "r"(kb) : "memory");
-            tc_commit(done_bar);
+            // every MMA issued above has completed before the teardown frees tensor memory
+            tc_commit(fin_bar);
+            mbar_wait(fin_bar, 0);
         }
         __syncwarp();
-    } else {
-        // converters: A -> A_hi in place, A_lo beside it
+    } else if (warp < 4) {
+        // ---- converters: A -> A_hi in place, A_lo beside it
         const int t = threadIdx.x - 64;
-        for (int kb = 0; kb < nk; ++kb) {
-            const int s = kb % kSplitStages, r = kb / kSplitStages;
-            if (!mbar_wait(full_bar(s), r & 1)) {
+        const long long total = static_cast<long long>(mine) * nk;
+        for (long long g = 0; g < total; ++g) {
+            const int s = static_cast<int>(g & 1);
+            if (!mbar_wait(full_bar(s), static_cast<uint32_t>((g >> 1) & 1))) {
                 atomicExch(err, 1);
                 break;
             }
@@ -462,49 +508,54 @@ __global__ void __launch_bounds__(128, 1)
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(conv_bar(s)) : "memory");
         }
-    }
-
-    const bool done = mbar_wait(done_bar, 0);
-    if (!done && threadIdx.x == 0) atomicExch(err, 1);
-    if (warp == 0 && lane == 0) {
-        int consumed;
-        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(consumed) : "r"(cslot) : "memory");
-        for (int kb = consumed; kb < issued; ++kb) mbar_wait(full_bar(kb % kSplitStages), (kb / kSplitStages) & 1);
-    }
-    tc_fence_after();
-    __syncthreads();
-    float* stile = reinterpret_cast<float*>(gbase);  // [128][kSplitBN + 1]
-    constexpr int kLd = kSplitBN + 1;
-    const int trow = warp * 32 + lane;
-    for (int c0 = 0; c0 < kSplitBN; c0 += 16) {
-        uint32_t v[16];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-            "%14, %15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int jj = 0; jj < 16; ++jj) stile[trow * kLd + c0 + jj] = __uint_as_float(v[jj]);
-    }
-    __syncthreads();
-    if (done) {
-        for (int cc = static_cast<int>(threadIdx.x); cc < kSplitBN; cc += 128) {
-            const int col = n0 + cc;
-            if (col >= N) break;
-            for (int rr = 0; rr < kBM; ++rr) {
-                const int row = m0 + rr;
-                if (row >= M) break;
-                out[static_cast<long long>(row) * ldo + col] = stile[rr * kLd + cc];
+    } else {
+        // ---- epilogue: warp 4 + q reads tensor-memory lanes (tile rows) 32 q .. 32 q + 31
+        const int q = warp - 4;
+        float* buf = reinterpret_cast<float*>(gbase + kSplitRing + q * kEpiBuf);  // [32][33]
+        for (int i = 0; i < mine; ++i) {
+            const int x = i & 1;
+            int m0, n0;
+            tile_of(i, m0, n0);
+            if (!mbar_wait(accf_bar(x), static_cast<uint32_t>((i >> 1) & 1))) {
+                atomicExch(err, 1);
+                break;
             }
+            tc_fence_after();
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(x * kSplitBN);
+            for (int c0 = 0; c0 < kSplitBN; c0 += 32) {
+                uint32_t v[32];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                    "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+                    "%30, %31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr + static_cast<uint32_t>(c0)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 32; ++j) buf[lane * 33 + j] = __uint_as_float(v[j]);
+                __syncwarp();
+                const int col = n0 + c0 + lane;
+                for (int rr = 0; rr < 32; ++rr) {
+                    const int row = m0 + q * 32 + rr;
+                    if (row < M && col < N) out[static_cast<long long>(row) * ldo + col] = buf[rr * 33 + lane];
+                }
+                __syncwarp();
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce_bar(x)) : "memory");
         }
     }
+
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kSplitBN)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kSplitBN)
                      : "memory");
     }
 }
@@ -646,7 +697,11 @@ bool tc_split_gemm(int M, int N, int K, const float* A, int lda, const float* Bh
         return false;
     const long long tiles = static_cast<long long>((N + kSplitBN - 1) / kSplitBN) * ((M + kBM - 1) / kBM);
     if (tiles > 0x7fffffffll) return false;
-    tc_split_gemm_kernel<<<static_cast<unsigned>(tiles), 128, kSplitSmem, s>>>(ma, mbh, mbl, M, N, K, out, ldo, err);
+    static int sms[64] = {};
+    if (sms[dev] == 0 && cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return false;
+    const unsigned grid = static_cast<unsigned>(tiles < sms[dev] ? tiles : sms[dev]);  // persistent: one CTA per SM
+    tc_split_gemm_kernel<<<grid, kSplitThreads, kSplitSmem, s>>>(ma, mbh, mbl, M, N, K, out, ldo, err);
     return true;
 }
 
