@@ -58,7 +58,7 @@ void release(hx_ctx* c)
                     c->up_slab, c->up_bath, c->U, c->vflip, c->Bbuf, c->rho32, c->ua32, c->ub32,
                     c->U32, c->diag32, c->vdiag32, c->hflip32, c->diag_herm, c->vbit, c->csr_ptr, c->csr_col,
                     c->csr_val, c->pack_scale, c->pack_bad, c->dense_hr, c->dense_hr_lo, c->dense_y,
-                    c->dense_h64, c->dense_z0};
+                    c->dense_h64, c->dense_z0, c->gbar};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -326,6 +326,15 @@ int enqueue_step(hx_ctx* c)
 {
     const int m = c->order;
     int launched = 0;
+    if (c->use_small_step && !c->closure) {
+        if (hx::launch_small_step(hx::fused_args_of(c), c->rho, c->ua, c->ub, c->dt, m, c->gbar, c->gbar + 1,
+                                  c->stream, false) != 1)
+            c->launch_failed = true;
+        c->counters.kernel_launches += 1;
+        c->counters.stage_launches += m;
+        c->steps_done += 1;
+        return HX_OK;
+    }
     if (m == 1) {
         launched += launch_stage_any(c, c->rho, c->rho, c->ua, c->dt, hx::kBaseSelf);
         std::swap(c->rho, c->ua);
@@ -372,6 +381,7 @@ int read_error_flag(hx_ctx* c)
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (flag != 0) {
         cudaMemsetAsync(c->error_flag, 0, sizeof(int), c->stream);
+        if (c->gbar) cudaMemsetAsync(c->gbar, 0, 2 * sizeof(unsigned), c->stream);  // a barrier that gave up
         return fail(HX_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration budget");
     }
     return HX_OK;
@@ -1048,6 +1058,16 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
             c->up_slots = S;
             c->use_fused = (rc == HX_OK) && fused_ok;
             c->use_small = (rc == HX_OK) && want_small;
+            // small slabs: the whole step in one cooperative launch when every ADO fits the resident CTAs
+            const char* step_env = std::getenv("HX_SMALL_STEP");
+            if (c->use_small && c->order >= 2 && !(step_env && step_env[0] == '0') &&
+                (rc = dev_alloc(c, &c->gbar, 2)) == HX_OK) {
+                e = cudaMemsetAsync(c->gbar, 0, 2 * sizeof(unsigned), c->stream);
+                if (e != cudaSuccess) rc = hx::cuda_fail(e, "grid barrier words");
+                else
+                    c->use_small_step = hx::launch_small_step(hx::fused_args_of(c), c->rho, c->ua, c->ub, c->dt,
+                                                              c->order, c->gbar, c->gbar + 1, c->stream, true) == 1;
+            }
             // single-precision copies of the operators for the mixed band kernel
             if (rc == HX_OK && c->mixed) {
                 if ((rc = dev_alloc(c, &c->diag32, c->slab)) || (rc = dev_alloc(c, &c->vdiag32, static_cast<size_t>(J) * d)) ||
@@ -1116,6 +1136,7 @@ int hx_ctx_info(const hx_ctx* c, hx_info* info)
     int per_stage = (c->use_flip || c->use_csr || (c->use_fused && c->up_slots > 0)) ? 2 : 1;
     if (c->use_large) per_stage = 1 + (c->up_slots > 0 ? 1 : 0) + (c->mixed ? 1 : 0) + (c->dense ? 2 : 0);
     info->kernels_per_step = static_cast<uint32_t>(c->order) * per_stage;
+    if (c->use_small_step && !c->closure) info->kernels_per_step = 1;
     info->stage_path = c->dense     ? HX_PATH_DENSE
                        : c->use_csr ? HX_PATH_CSR
                        : c->use_flip ? HX_PATH_FLIP

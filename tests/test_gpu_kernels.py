@@ -1,8 +1,10 @@
 """The small-slab stage kernels against the oracle: small_kernel (hx_small.cu,
 d <= 16 with sigma_z couplings, batched neighbour gathers; the default for
-those shapes) and the generic stage_kernel it replaces there
-(HX_SMALL_STAGE=0).  RHS within 1e-12 relative and trajectories within 1e-10
-max-abs, the tolerances of the other parity tests."""
+those shapes), its one-launch-per-step form small_step_kernel (the stages of
+a step separated by grid barriers; HX_SMALL_STEP=0 selects one launch per
+stage) and the generic stage_kernel they replace (HX_SMALL_STAGE=0).  RHS
+within 1e-12 relative and trajectories within 1e-10 max-abs, the tolerances
+of the other parity tests; the two small forms give the same bits."""
 import numpy as np
 import pytest
 
@@ -46,3 +48,28 @@ def test_small_kernel_c1_trajectory(monkeypatch):
         rho, en = ctx.step_trace(steps)
     assert np.max(np.abs(rho - rho_ref)) <= TOL
     assert np.max(np.abs(en - en_ref)) <= TOL
+
+
+@pytest.mark.parametrize("n,depth,K,order", [(4, 3, 2, 4), (4, 3, 3, 4), (2, 3, 2, 4), (3, 4, 2, 3), (4, 2, 2, 2)])
+def test_small_step_kernel_matches_stage_launches(monkeypatch, n, depth, K, order):
+    """One launch per step against one launch per stage: identical states
+    after 25 steps (the per-ADO arithmetic is the same), including 969 ADOs
+    at d = 16 (several ADOs per CTA) and Horner orders 2 and 3."""
+    monkeypatch.setenv("HX_SMALL_STAGE", "1")
+    p = S.spin_glass(n, seed=300 + n + depth, depth=depth, K=K, h=0.9, dt=0.01)
+    steps = 25
+    out = {}
+    for form in ("step", "stage"):
+        monkeypatch.setenv("HX_SMALL_STEP", "1" if form == "step" else "0")
+        with capi.Context(p, order=order) as ctx:
+            assert ctx.stage_path == "small"
+            kps = ctx.get_info().kernels_per_step
+            assert kps == (1 if form == "step" else order)
+            rho, en = ctx.step_trace(steps)
+            out[form] = (rho, en, ctx.state())
+    for a, b in zip(out["step"], out["stage"]):
+        assert np.array_equal(a, b)
+    o = O.Oracle(p)
+    rho_ref, _ = o.run(5, order=order, trace=True)
+    o.close()
+    assert np.max(np.abs(out["step"][0][:5] - rho_ref)) <= TOL
