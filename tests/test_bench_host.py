@@ -60,9 +60,18 @@ def test_clock_sampler_reports_its_fields():
     assert isinstance(r["reasons"], list)
 
 
+class _Info:
+    def __init__(self, kps):
+        self.kernels_per_step = kps
+
+
 class _Ctx:
-    def __init__(self, path):
+    def __init__(self, path, kps=4):
         self.stage_path = path
+        self._kps = kps
+
+    def get_info(self):
+        return _Info(self._kps)
 
 
 @pytest.mark.parametrize("path,packed,per_stage,want", [
@@ -76,3 +85,9 @@ class _Ctx:
 def test_stage_kernel_labels(path, packed, per_stage, want):
     p = S.spin_glass(6, seed=1, depth=1, K=1)
     assert bench.stage_kernels_label(_Ctx(path), p, packed, per_stage) == want
+
+
+def test_step_kernel_label():
+    p = S.spin_glass(4, seed=1, depth=1, K=1)
+    label = bench.stage_kernels_label(_Ctx("small", kps=1), p, False, 1)
+    assert label.startswith("small_step_kernel per step")
