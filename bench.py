@@ -247,7 +247,7 @@ def stage_kernels_label(ctx, p, packed: bool, per_stage: int) -> str:
         return k + (" + upterm_kernel" if per_stage == 2 else "") + " per stage" + \
             (" (Hermitian-packed slabs)" if packed else "")
     if path == "small":
-        if int(ctx.get_info().kernels_per_step) == 1:
+        if int(ctx.info.kernels_per_step) == 1:
             return "small_step_kernel per step (d <= 16; the 4 stages in one cooperative launch, grid barriers)"
         return "small_kernel per stage (d <= 16, batched neighbour gathers)"
     return "stage_kernel per stage (generic path)"
@@ -484,7 +484,7 @@ def run_ours(args, cfg: dict) -> None:
     stages = 4
     alg_bytes_per_step = (3 * stages - 1) * state_bytes
     # launches per step: one per stage, or one for the whole step (small_step_kernel)
-    step_launch = ctx.stage_path == "small" and int(ctx.get_info().kernels_per_step) == 1
+    step_launch = ctx.stage_path == "small" and int(ctx.info.kernels_per_step) == 1
     launches_per_step = 1 if step_launch else stages
     per_launch_bytes = alg_bytes_per_step / launches_per_step
     launch_ms = ms / (args.steps * launches_per_step)

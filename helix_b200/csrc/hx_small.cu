@@ -132,33 +132,31 @@ void launch_small_t(const FusedArgs& a, const double2* u, const double2* rho, do
 }
 
 // Grid barrier of small_step_kernel: every CTA is resident (cooperative
-// launch).  The block's writes are ordered before thread 0's arrival by the
-// block barrier and a GPU-scope fence; the last CTA to arrive resets the
-// count and advances the generation, the others wait (bounded) for the
-// generation to move.  Returns false when the wait ran out.
-__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned G)
+// launch).  One monotonic arrival counter: barrier k of a launch waits until
+// the counter reaches base + (k + 1) G, base being its value when the launch
+// began (the host keeps count of the barriers taken).  The block's writes are
+// ordered before thread 0's arrival by the block barrier and a GPU-scope
+// fence; the wait polls the counter with acquire loads, bounded.  Returns
+// false when the wait ran out.
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned target)
 {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        const unsigned g0 = *reinterpret_cast<volatile unsigned*>(gen);
         __threadfence();
-        if (atomicAdd(count, 1u) == G - 1) {
-            *reinterpret_cast<volatile unsigned*>(count) = 0u;
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
-            uint32_t it = 0;
-            while (*reinterpret_cast<volatile unsigned*>(gen) == g0) {
-                if (++it > (1u << 24)) {
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(20);
+        atomicAdd(count, 1u);
+        uint32_t it = 0;
+        while (true) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+            if (static_cast<int>(v - target) >= 0) break;
+            if (++it > (1u << 24)) {
+                ok = 0;
+                break;
             }
+            __nanosleep(20);
         }
-        __threadfence();
     }
     __syncthreads();
     return ok != 0;
@@ -180,7 +178,7 @@ constexpr int kStepPer = 4;
 template <int LOGD, int MAXPER>
 __global__ void __launch_bounds__((1 << (2 * LOGD)) < 32 ? 32 : (1 << (2 * LOGD)), MAXPER == 1 ? 4 : 2)
     small_step_kernel(FusedArgs a, double2* rho, double2* ua, double2* ub, double dt, int order, int per,
-                      unsigned* gcount, unsigned* ggen)
+                      unsigned* gcount, unsigned gbase)
 {
     constexpr int D = 1 << LOGD, D2 = D * D;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -290,7 +288,7 @@ __global__ void __launch_bounds__((1 << (2 * LOGD)) < 32 ? 32 : (1 << (2 * LOGD)
             out[nn[j] * D2 + e] = o;
             x[j] = o;
         }
-        if (st < order && !grid_barrier(gcount, ggen, G)) {
+        if (st < order && !grid_barrier(gcount, gbase + static_cast<unsigned>(st) * G)) {
             if (tid == 0) atomicExch(a.error_flag, 1);
             return;
         }
@@ -300,7 +298,7 @@ __global__ void __launch_bounds__((1 << (2 * LOGD)) < 32 ? 32 : (1 << (2 * LOGD)
 
 template <int LOGD, int MAXPER>
 int launch_small_step_v(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                        unsigned* gcount, unsigned* ggen, cudaStream_t s, bool dry)
+                        unsigned* gcount, unsigned gbase, cudaStream_t s, bool dry, int* ctas)
 {
     // 1 launched (or would launch, dry), 0 the ADOs do not fit (try the next form), -1 refused
     constexpr int D2 = 1 << (2 * LOGD);
@@ -323,10 +321,11 @@ int launch_small_step_v(const FusedArgs& a, double2* rho, double2* ua, double2* 
         if (capacity[dev][per] < 0) return -1;
         const long long grid = (a.H + per - 1) / per;
         if (grid > capacity[dev][per]) continue;
+        if (ctas) *ctas = static_cast<int>(grid);
         if (dry) return 1;
         FusedArgs args = a;
         int per_arg = per;
-        void* params[] = {&args, &rho, &ua, &ub, &dt, &order, &per_arg, &gcount, &ggen};
+        void* params[] = {&args, &rho, &ua, &ub, &dt, &order, &per_arg, &gcount, &gbase};
         return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(small_step_kernel<LOGD, MAXPER>),
                                            dim3(static_cast<unsigned>(grid)), dim3(threads), params, smem,
                                            s) == cudaSuccess
@@ -338,11 +337,11 @@ int launch_small_step_v(const FusedArgs& a, double2* rho, double2* ua, double2* 
 
 template <int LOGD>
 int launch_small_step_t(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                        unsigned* gcount, unsigned* ggen, cudaStream_t s, bool dry)
+                        unsigned* gcount, unsigned gbase, cudaStream_t s, bool dry, int* ctas)
 {
-    const int r1 = launch_small_step_v<LOGD, 1>(a, rho, ua, ub, dt, order, gcount, ggen, s, dry);
+    const int r1 = launch_small_step_v<LOGD, 1>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
     if (r1 != 0) return r1;
-    return launch_small_step_v<LOGD, kStepPer>(a, rho, ua, ub, dt, order, gcount, ggen, s, dry);
+    return launch_small_step_v<LOGD, kStepPer>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
 }
 
 }  // namespace
@@ -362,14 +361,14 @@ size_t small_step_smem(int logd, int M, int per)
 }
 
 int launch_small_step(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                      unsigned* gcount, unsigned* ggen, cudaStream_t s, bool dry)
+                      unsigned* gcount, unsigned gbase, cudaStream_t s, bool dry, int* ctas)
 {
     if (order < 2) return 0;  // order 1 writes rho while neighbours read it
     switch (a.logd) {
-    case 1: return launch_small_step_t<1>(a, rho, ua, ub, dt, order, gcount, ggen, s, dry);
-    case 2: return launch_small_step_t<2>(a, rho, ua, ub, dt, order, gcount, ggen, s, dry);
-    case 3: return launch_small_step_t<3>(a, rho, ua, ub, dt, order, gcount, ggen, s, dry);
-    case 4: return launch_small_step_t<4>(a, rho, ua, ub, dt, order, gcount, ggen, s, dry);
+    case 1: return launch_small_step_t<1>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
+    case 2: return launch_small_step_t<2>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
+    case 3: return launch_small_step_t<3>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
+    case 4: return launch_small_step_t<4>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
     default: return 0;
     }
 }

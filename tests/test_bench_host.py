@@ -68,10 +68,7 @@ class _Info:
 class _Ctx:
     def __init__(self, path, kps=4):
         self.stage_path = path
-        self._kps = kps
-
-    def get_info(self):
-        return _Info(self._kps)
+        self.info = _Info(kps)  # capi.Context keeps the hx_info of its creation (valid after close)
 
 
 @pytest.mark.parametrize("path,packed,per_stage,want", [
