@@ -225,7 +225,8 @@ def test_state_roundtrip_and_counters():
         ctx.sync()
         assert ctx.counters().stage_launches - c0 == 3 * 4
         info = ctx.get_info()
-        assert info.steps_done == 3 and info.kernels_per_step == 4
+        # d = 8 with sigma_z couplings: the whole step is one launch of small_step_kernel
+        assert info.steps_done == 3 and info.kernels_per_step == 1
 
 
 def test_initial_state_and_energy():
