@@ -1283,11 +1283,72 @@ int hx_ctx_read_state(hx_ctx* c, double* out, uint64_t n)
     return read_error_flag(c);
 }
 
+namespace {
+
+constexpr int kNoStaging = -1;
+
+// Mixed precision: upload the FP64 state into a temporary device buffer, check
+// Hermiticity there when the context needs it (packed slabs, or a dense H),
+// and convert (and pack) on the device.  kNoStaging when the temporary buffer
+// cannot be had; the caller then converts on the host.
+int write_state_mixed_device(hx_ctx* c, const double* in)
+{
+    const size_t count = static_cast<size_t>(c->H) * c->slab;
+    double2* stage = nullptr;
+    if (cudaMalloc(&stage, count * sizeof(double2)) != cudaSuccess) {
+        cudaGetLastError();  // clear the allocation failure
+        return kNoStaging;
+    }
+    auto done = [&](int rc) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(stage);
+        return rc;
+    };
+    cudaError_t e = cudaMemcpyAsync(stage, in, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return done(hx::cuda_fail(e, "state upload"));
+    c->counters.h2d_bytes += count * sizeof(double2);
+    if (c->herm || c->dense) {
+        int rc = HX_OK;
+        if (!c->pack_scale && ((rc = dev_alloc(c, &c->pack_scale, c->H)) || (rc = dev_alloc(c, &c->pack_bad, 1))))
+            return done(rc);
+        e = cudaMemsetAsync(c->pack_bad, 0x7f, sizeof(int), c->stream);
+        if (e != cudaSuccess) return done(hx::cuda_fail(e, "state check"));
+        hx::launch_herm_check(stage, c->H, c->logd, 1e-12, c->pack_scale, 0, c->pack_bad, c->stream);
+        int bad = 0;
+        e = cudaMemcpyAsync(&bad, c->pack_bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return done(hx::cuda_fail(e, "state check"));
+        if (bad != 0x7f7f7f7f)
+            return done(fail(HX_ERR_INVALID_RUNTIME_OPTION,
+                             "ADO " + std::to_string(bad) +
+                                 (c->dense ? " is not Hermitian, which HX_FLAG_DENSE_H requires"
+                                           : " is not Hermitian; this context keeps Hermitian-packed slabs (create it "
+                                             "with HX_FLAG_FULL_STATE for general states)")));
+    }
+    if (c->herm) {
+        hx::launch_herm_pack_f32(stage, c->H, c->logd, 0, c->rho32, c->stream);
+        hx::launch_herm_pack(stage, 1, c->logd, 0, c->rho, c->stream);
+    } else {
+        hx::launch_d2f(stage, c->rho32, static_cast<long long>(count), c->stream);
+        e = cudaMemcpyAsync(c->rho, stage, c->slab * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream);
+        if (e != cudaSuccess) return done(hx::cuda_fail(e, "state upload"));
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return done(hx::cuda_fail(e, "state conversion"));
+    return done(HX_OK);
+}
+
+}  // namespace
+
 int hx_ctx_write_state(hx_ctx* c, const double* in, uint64_t n)
 {
     if (!c || !in) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
     const size_t count = static_cast<size_t>(c->H) * c->slab;
     if (n < 2 * count) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "input buffer too small");
+    if (c->mixed) {
+        const int rc = write_state_mixed_device(c, in);
+        if (rc != kNoStaging) return rc;
+    }
     if (c->mixed && c->herm) {
         const size_t P = c->slab_store;
         std::vector<double2> pk(static_cast<size_t>(c->H) * P);

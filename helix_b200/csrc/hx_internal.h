@@ -120,6 +120,9 @@ void launch_herm_check(const double2* full, long long count, int logd, double re
                        long long first, int* bad, cudaStream_t s);
 void launch_herm_pack(const double2* full, long long count, int logd, long long first, double2* packed,
                       cudaStream_t s);
+// The same packing into complex64 slabs (mixed precision).
+void launch_herm_pack_f32(const double2* full, long long count, int logd, long long first, float2* packed,
+                          cudaStream_t s);
 // Full row-major complex matrix (2 d^2 doubles) from a packed slab, on the host.
 void unpack_herm_host(const double2* pk, int logd, double* out);
 

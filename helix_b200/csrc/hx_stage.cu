@@ -367,6 +367,31 @@ void launch_herm_check(const double2* full, long long count, int logd, double re
     pack_check_kernel<<<148 * 8, 256, 0, s>>>(full, count, logd, rel_tol * rel_tol, scale2, first, nullptr, bad);
 }
 
+// Packed complex64 copy of `count` full FP64 slabs (the mixed-precision hierarchy's upload).
+__global__ void pack_f32_kernel(const double2* __restrict__ full, long long count, int logd, long long first,
+                                float2* __restrict__ packed)
+{
+    const int D = 1 << logd;
+    const long long P = herm_elems(logd);
+    const long long total = count * P;
+    for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long k = t / P;
+        const int i = static_cast<int>(t - k * P);
+        int r, c;
+        herm_coords(i, logd, r, c);
+        const double2 up = full[k * static_cast<long long>(D) * D + static_cast<long long>(r) * D + c];
+        packed[(first + k) * P + i] = make_float2(static_cast<float>(up.x), static_cast<float>(up.y));
+    }
+}
+
+void launch_herm_pack_f32(const double2* full, long long count, int logd, long long first, float2* packed,
+                          cudaStream_t s)
+{
+    if (count <= 0) return;
+    pack_f32_kernel<<<148 * 8, 256, 0, s>>>(full, count, logd, first, packed);
+}
+
 void launch_herm_pack(const double2* full, long long count, int logd, long long first, double2* packed,
                       cudaStream_t s)
 {
