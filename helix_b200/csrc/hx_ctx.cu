@@ -327,11 +327,8 @@ int enqueue_step(hx_ctx* c)
     const int m = c->order;
     int launched = 0;
     if (c->use_small_step && !c->closure) {
-        const unsigned base = static_cast<unsigned>(c->gbar_taken * static_cast<uint64_t>(c->step_ctas));
-        if (hx::launch_small_step(hx::fused_args_of(c), c->rho, c->ua, c->ub, c->dt, m, c->gbar, base, c->stream,
-                                  false) != 1)
+        if (hx::launch_small_step(hx::fused_args_of(c), c->rho, c->ua, c->ub, c->dt, m, c->gbar, c->stream, false) != 1)
             c->launch_failed = true;
-        c->gbar_taken += static_cast<uint64_t>(m - 1);
         c->counters.kernel_launches += 1;
         c->counters.stage_launches += m;
         c->steps_done += 1;
@@ -383,10 +380,7 @@ int read_error_flag(hx_ctx* c)
     HX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (flag != 0) {
         cudaMemsetAsync(c->error_flag, 0, sizeof(int), c->stream);
-        if (c->gbar) {  // a barrier that gave up leaves the arrival count behind: start it again
-            cudaMemsetAsync(c->gbar, 0, sizeof(unsigned), c->stream);
-            c->gbar_taken = 0;
-        }
+        if (c->gbar) cudaMemsetAsync(c->gbar, 0, sizeof(unsigned), c->stream);  // a barrier that gave up
         return fail(HX_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration budget");
     }
     return HX_OK;
@@ -1071,8 +1065,7 @@ int hx_ctx_create(const hx_problem* p, hx_ctx** out)
                 if (e != cudaSuccess) rc = hx::cuda_fail(e, "grid barrier counter");
                 else
                     c->use_small_step = hx::launch_small_step(hx::fused_args_of(c), c->rho, c->ua, c->ub, c->dt,
-                                                              c->order, c->gbar, 0, c->stream, true,
-                                                              &c->step_ctas) == 1;
+                                                              c->order, c->gbar, c->stream, true) == 1;
             }
             // single-precision copies of the operators for the mixed band kernel
             if (rc == HX_OK && c->mixed) {

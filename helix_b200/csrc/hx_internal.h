@@ -191,13 +191,12 @@ void launch_transpose_bf16(const void* in, int rows, int cols, int ld_in, void* 
 size_t small_smem(int logd, int M);
 bool small_supported(int logd, int M, int pauli);
 // The same, one cooperative launch per integrator step (order >= 2), stages separated by grid barriers on
-// a monotonic arrival counter (*gcount, zeroed by the caller once; gbase = its value at the launch, i.e.
-// the barriers taken so far x the launch's CTAs, which small_step_ctas gives).  Returns 1 when launched
-// (with dry: when it would launch), 0 when the ADOs do not fit the resident CTAs (up to 4 per CTA), -1
-// when refused.
+// an arrival counter (*gcount, zeroed by the caller once; every launch leaves it at zero).  Returns 1 when
+// launched (with dry: when it would launch), 0 when the ADOs do not fit the resident CTAs (up to 4 per
+// CTA), -1 when refused.
 size_t small_step_smem(int logd, int M, int per);
 int launch_small_step(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                      unsigned* gcount, unsigned gbase, cudaStream_t s, bool dry, int* ctas = nullptr);
+                      unsigned* gcount, cudaStream_t s, bool dry);
 bool launch_small(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
                   int base_kind, cudaStream_t s);
 bool prepare_fused(int logd, int M, int J, int herm);  // raises the shared-memory limit; call before stream capture
@@ -414,8 +413,6 @@ struct hx_ctx {
     bool use_small = false;       // d <= 16 sigma_z stage kernel (hx_small.cu)
     bool use_small_step = false;  // ... as one cooperative launch per step (small_step_kernel)
     unsigned* gbar = nullptr;     // grid-barrier arrival counter of small_step_kernel
-    uint64_t gbar_taken = 0;      // grid barriers taken so far (the counter's base, in units of the CTAs)
-    int step_ctas = 0;            // CTAs of a small_step_kernel launch
     int sm_count = 0;
     int up_slots = 0;             // ADOs in tier L-1
     int32_t* up_slot = nullptr;   // [H]

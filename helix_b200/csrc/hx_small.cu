@@ -132,12 +132,13 @@ void launch_small_t(const FusedArgs& a, const double2* u, const double2* rho, do
 }
 
 // Grid barrier of small_step_kernel: every CTA is resident (cooperative
-// launch).  One monotonic arrival counter: barrier k of a launch waits until
-// the counter reaches base + (k + 1) G, base being its value when the launch
-// began (the host keeps count of the barriers taken).  The block's writes are
-// ordered before thread 0's arrival by the block barrier and a GPU-scope
-// fence; the wait polls the counter with acquire loads, bounded.  Returns
-// false when the wait ran out.
+// launch).  One arrival counter, zero when a launch begins: barrier k of the
+// launch waits until it reaches (k + 1) G.  The block's writes are ordered
+// before thread 0's arrival by the block barrier and a GPU-scope fence; the
+// wait polls the counter with acquire loads, bounded.  After its last stage
+// every CTA arrives once more and the last to do so puts the counter back to
+// zero, so no host-side count is involved (a captured launch replays
+// correctly).  Returns false when the wait ran out.
 __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned target)
 {
     __shared__ int ok;
@@ -178,7 +179,7 @@ constexpr int kStepPer = 4;
 template <int LOGD, int MAXPER>
 __global__ void __launch_bounds__((1 << (2 * LOGD)) < 32 ? 32 : (1 << (2 * LOGD)), MAXPER == 1 ? 4 : 2)
     small_step_kernel(FusedArgs a, double2* rho, double2* ua, double2* ub, double dt, int order, int per,
-                      unsigned* gcount, unsigned gbase)
+                      unsigned* gcount)
 {
     constexpr int D = 1 << LOGD, D2 = D * D;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -288,17 +289,19 @@ __global__ void __launch_bounds__((1 << (2 * LOGD)) < 32 ? 32 : (1 << (2 * LOGD)
             out[nn[j] * D2 + e] = o;
             x[j] = o;
         }
-        if (st < order && !grid_barrier(gcount, gbase + static_cast<unsigned>(st) * G)) {
+        if (st < order && !grid_barrier(gcount, static_cast<unsigned>(st) * G)) {
             if (tid == 0) atomicExch(a.error_flag, 1);
             return;
         }
         in = out;
     }
+    // every CTA has passed every barrier: the last one to get here resets the counter for the next launch
+    if (tid == 0 && atomicAdd(gcount, 1u) == static_cast<unsigned>(order) * G - 1u) atomicExch(gcount, 0u);
 }
 
 template <int LOGD, int MAXPER>
 int launch_small_step_v(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                        unsigned* gcount, unsigned gbase, cudaStream_t s, bool dry, int* ctas)
+                        unsigned* gcount, cudaStream_t s, bool dry)
 {
     // 1 launched (or would launch, dry), 0 the ADOs do not fit (try the next form), -1 refused
     constexpr int D2 = 1 << (2 * LOGD);
@@ -321,11 +324,10 @@ int launch_small_step_v(const FusedArgs& a, double2* rho, double2* ua, double2* 
         if (capacity[dev][per] < 0) return -1;
         const long long grid = (a.H + per - 1) / per;
         if (grid > capacity[dev][per]) continue;
-        if (ctas) *ctas = static_cast<int>(grid);
         if (dry) return 1;
         FusedArgs args = a;
         int per_arg = per;
-        void* params[] = {&args, &rho, &ua, &ub, &dt, &order, &per_arg, &gcount, &gbase};
+        void* params[] = {&args, &rho, &ua, &ub, &dt, &order, &per_arg, &gcount};
         return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(small_step_kernel<LOGD, MAXPER>),
                                            dim3(static_cast<unsigned>(grid)), dim3(threads), params, smem,
                                            s) == cudaSuccess
@@ -337,11 +339,11 @@ int launch_small_step_v(const FusedArgs& a, double2* rho, double2* ua, double2* 
 
 template <int LOGD>
 int launch_small_step_t(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                        unsigned* gcount, unsigned gbase, cudaStream_t s, bool dry, int* ctas)
+                        unsigned* gcount, cudaStream_t s, bool dry)
 {
-    const int r1 = launch_small_step_v<LOGD, 1>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
+    const int r1 = launch_small_step_v<LOGD, 1>(a, rho, ua, ub, dt, order, gcount, s, dry);
     if (r1 != 0) return r1;
-    return launch_small_step_v<LOGD, kStepPer>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
+    return launch_small_step_v<LOGD, kStepPer>(a, rho, ua, ub, dt, order, gcount, s, dry);
 }
 
 }  // namespace
@@ -361,14 +363,14 @@ size_t small_step_smem(int logd, int M, int per)
 }
 
 int launch_small_step(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                      unsigned* gcount, unsigned gbase, cudaStream_t s, bool dry, int* ctas)
+                      unsigned* gcount, cudaStream_t s, bool dry)
 {
     if (order < 2) return 0;  // order 1 writes rho while neighbours read it
     switch (a.logd) {
-    case 1: return launch_small_step_t<1>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
-    case 2: return launch_small_step_t<2>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
-    case 3: return launch_small_step_t<3>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
-    case 4: return launch_small_step_t<4>(a, rho, ua, ub, dt, order, gcount, gbase, s, dry, ctas);
+    case 1: return launch_small_step_t<1>(a, rho, ua, ub, dt, order, gcount, s, dry);
+    case 2: return launch_small_step_t<2>(a, rho, ua, ub, dt, order, gcount, s, dry);
+    case 3: return launch_small_step_t<3>(a, rho, ua, ub, dt, order, gcount, s, dry);
+    case 4: return launch_small_step_t<4>(a, rho, ua, ub, dt, order, gcount, s, dry);
     default: return 0;
     }
 }

@@ -73,3 +73,32 @@ def test_small_step_kernel_matches_stage_launches(monkeypatch, n, depth, K, orde
     rho_ref, _ = o.run(5, order=order, trace=True)
     o.close()
     assert np.max(np.abs(out["step"][0][:5] - rho_ref)) <= TOL
+
+
+def test_small_step_kernel_replays_from_a_captured_graph(monkeypatch):
+    """The step kernel's grid barrier keeps no host-side count: a CUDA graph
+    captured from one hx_ctx_step replays into the same states as steps
+    launched one by one."""
+    import torch
+
+    monkeypatch.setenv("HX_SMALL_STAGE", "1")
+    monkeypatch.setenv("HX_SMALL_STEP", "1")
+    p = S.spin_glass(4, seed=2024, depth=3, K=2, h=1.0, dt=0.01)
+    steps = 7
+    with capi.Context(p) as ref:
+        assert ref.get_info().kernels_per_step == 1
+        ref.step(steps)
+        want = ref.state()
+    stream = torch.cuda.Stream()
+    with capi.Context(p) as ctx:
+        ctx.set_stream(stream.cuda_stream)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            ctx.step(1)
+        for _ in range(steps):
+            graph.replay()
+        torch.cuda.synchronize()
+        ctx.sync()
+        got = ctx.state()
+        del graph
+    assert np.array_equal(got, want)
