@@ -227,3 +227,40 @@ def test_closure_term_is_the_network_on_the_documented_features():
     assert np.max(np.abs(want)) > 0
     assert np.max(np.abs(diff - want)) <= 1e-10 * max(1.0, np.max(np.abs(want)))
     cl.close()
+
+
+def test_closure_at_the_c5_size():
+    """The C5 shape: d = 32 (5 spins), Pade K = 2 (15 modes), L = 2 closed
+    against L = 5, hidden width 512, 1000-step trajectories sampled every 50
+    steps; 8 training seeds (the bench uses 64) and 2 held-out seeds.  The
+    closure must cut the truncation error (max over the trajectory of the rho_0
+    trace distance to L = 5) on every held-out seed, and at least 2x on
+    average."""
+    n, K, steps, every = 5, 2, 1000, 50
+    coarse_depth, fine_depth = 2, 5
+    train_seeds, test_seeds = [5000 + s for s in range(8)], [9000, 9001]
+
+    def problem(seed, depth):
+        return S.spin_glass(n, seed=seed, depth=depth, K=K, h=1.0, dt=0.01)
+
+    cl = capi.Closure(problem(train_seeds[0], coarse_depth), fine_max_depth=fine_depth + 1, hidden=512,
+                      capacity=len(train_seeds) * steps // every, seed=1)
+    for s in train_seeds:
+        with capi.Context(problem(s, fine_depth)) as ctx:
+            for _ in range(steps // every):
+                ctx.step(every)
+                cl.harvest(ctx)
+    trace = cl.train(iters=1500, batch=8192, lr=3e-3, seed=7)
+    assert np.all(np.isfinite(trace))
+    gains = []
+    for s in test_seeds:
+        ref = _rho_traj(problem(s, fine_depth), steps)
+        plain = _rho_traj(problem(s, coarse_depth), steps)
+        closed = _rho_traj(problem(s, coarse_depth), steps, closure=cl)
+        e_plain = max(_trace_distance(plain[t], ref[t]) for t in range(0, steps, 10))
+        e_closed = max(_trace_distance(closed[t], ref[t]) for t in range(0, steps, 10))
+        assert e_closed < e_plain, (s, e_closed, e_plain)
+        gains.append(e_plain / e_closed)
+    print(f"closure gains at the C5 size: {gains}")
+    assert np.mean(gains) >= 2.0, gains
+    cl.close()
