@@ -518,6 +518,17 @@ public:
             p.precision = HX_PRECISION_MIXED;
             rc = hx_ctx_create(&p, &ctx_);
             mixed_ = rc == HX_OK;
+            // an H given as CSR with many entries per row (16 or more on average) and outside the
+            // diagonal-plus-flip form: single precision with the commutator on the tensor cores
+            if (rc == HX_ERR_UNSUPPORTED_PRECISION && sys.h_is_csr && sys.hcsr.col.size() >= 16 * std::size_t(sys.dim)) {
+                p.flags = HX_FLAG_FULL_STATE | HX_FLAG_DENSE_H;
+                rc = hx_ctx_create(&p, &ctx_);
+                mixed_ = rc == HX_OK;
+                if (rc != HX_OK) {
+                    p.flags = 0;
+                    rc = HX_ERR_UNSUPPORTED_PRECISION;
+                }
+            }
         }
         if (rc == HX_ERR_UNSUPPORTED_PRECISION) {
             p.precision = HX_PRECISION_DOUBLE;

@@ -2,11 +2,12 @@
 // (helix::HEOMSolver(options).run(system, hierarchy, solverOptions)) and
 // prints the result as JSON for tests/test_cpp_api.py to check against the
 // FP64 oracle.  Usage: api_spin_glass <spins> <seed> <h> <depth> <K> <steps> <dt> <mode>
-//   mode: final | trace | trajectory | single | legacy | sparse-bad | sparse-general
+//   mode: final | trace | trajectory | single | legacy | sparse-bad | sparse-general | dense-single
 #include <helix/helix.h>
 
 #include <algorithm>
 #include <complex>
+#include <cmath>
 #include <cstdio>
 #include <utility>
 #include <vector>
@@ -60,6 +61,33 @@ int main(int argc, char** argv)
             for (const auto& e : row) {
                 H.columnIndices.push_back(e.first);
                 H.values.push_back(e.second);
+            }
+            H.rowOffsets.push_back(H.columnIndices.size());
+        }
+        system = helix::System::from_sparse(H, system.couplings);
+    }
+    if (mode == "dense-single") {
+        // H plus a dense Hermitian term (every entry non-zero), single precision requested: the
+        // mixed-precision path with the commutator on the tensor cores
+        options.precision = helix::Precision::Single;
+        const helix::SparseOperator& H0 = system.hamiltonian;
+        const std::size_t d = H0.rows;
+        std::vector<std::complex<double>> dense(d * d);
+        for (std::size_t r = 0; r < d; ++r)
+            for (std::size_t p = H0.rowOffsets[r]; p < H0.rowOffsets[r + 1]; ++p) dense[r * d + H0.columnIndices[p]] += H0.values[p];
+        const double scale = 0.02 / std::sqrt(static_cast<double>(d));
+        for (std::size_t r = 0; r < d; ++r)
+            for (std::size_t c = 0; c < d; ++c) {
+                const double a = 0.3 * r + 0.7 * c, b = 0.3 * c + 0.7 * r;
+                dense[r * d + c] += scale * std::complex<double>(std::cos(a) + std::cos(b), std::sin(a) - std::sin(b));
+            }
+        helix::SparseOperator H;
+        H.rows = H.cols = d;
+        H.rowOffsets.assign(1, 0);
+        for (std::size_t r = 0; r < d; ++r) {
+            for (std::size_t c = 0; c < d; ++c) {
+                H.columnIndices.push_back(c);
+                H.values.push_back(dense[r * d + c]);
             }
             H.rowOffsets.push_back(H.columnIndices.size());
         }

@@ -131,3 +131,32 @@ def test_cpp_api_runs_the_reference_example(exe):
     o.close()
     assert np.max(np.abs(rho - want)) <= 1e-10
     assert abs(r["energies"][0] - e_ref) <= 1e-10
+
+
+@pytest.mark.gpu
+def test_cpp_api_single_precision_with_a_dense_hamiltonian(exe):
+    """System::from_sparse with a dense H (every entry non-zero) and
+    Precision::Single: the mixed path with the commutator on the tensor cores
+    (HX_FLAG_DENSE_H); rho0 within trace distance 1e-6 of the FP64 oracle given
+    the same operator."""
+    spins, seed, h, depth, K, steps, dt = 7, 2031, 0.5, 2, 1, 10, 0.005
+    r = _run(exe, spins, seed, h, depth, K, steps, dt, "dense-single")
+    assert r["ok"], r["codes"]
+    assert r["single"] is True
+    p = S.spin_glass(spins, seed=seed, depth=depth, K=K, h=h, dt=dt)
+    d = p.dim
+    m = p.h_dense()
+    rr, cc = np.meshgrid(np.arange(d), np.arange(d), indexing="ij")
+    a, b = 0.3 * rr + 0.7 * cc, 0.3 * cc + 0.7 * rr
+    m = m + (0.02 / np.sqrt(d)) * ((np.cos(a) + np.cos(b)) + 1j * (np.sin(a) - np.sin(b)))
+    p.h_csr_explicit = (np.arange(0, d * d + 1, d, dtype=np.int32), np.tile(np.arange(d, dtype=np.int32), d),
+                        m.reshape(-1).copy())
+    o = O.Oracle(p)
+    o.run(steps)
+    want, e_ref = o.rho0(), o.energy()
+    o.close()
+    rho = np.array(r["rho"]).view(np.complex128).reshape(d, d)
+    diff = rho - want
+    td = 0.5 * float(np.sum(np.abs(np.linalg.eigvalsh(0.5 * (diff + diff.conj().T)))))
+    assert td <= 1e-6, td
+    assert abs(r["energies"][0] - e_ref) <= 1e-6
