@@ -114,6 +114,10 @@ def test_dense_rejects_non_hermitian_states_and_unsupported_shapes():
     with pytest.raises(capi.HxError) as e:
         capi.Context(p, dense_h=True)  # double precision
     assert e.value.status == "UnsupportedExecution"
+    with capi.Context(S.spin_glass(7, seed=1, depth=2, K=1), precision="mixed") as plain:  # not a dense-H context
+        with pytest.raises(capi.HxError) as e:
+            plain.dense_product(1)
+        assert e.value.status == "UnsupportedExecution"
     with pytest.raises(capi.HxError) as e:
         capi.Context(S.dense_h_problem(6, seed=1, depth=2, K=1, n_baths=2), precision="mixed", dense_h=True)
     assert e.value.status in ("UnsupportedExecution", "UnsupportedPrecision")
