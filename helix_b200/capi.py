@@ -34,7 +34,7 @@ EXPORTS = [
     "hx_seeded_couplings", "hx_ctx_create", "hx_ctx_destroy", "hx_ctx_set_stream", "hx_ctx_get_stream",
     "hx_ctx_info", "hx_ctx_counters", "hx_ctx_step", "hx_ctx_step_trace", "hx_ctx_sync",
     "hx_ctx_read_rho0", "hx_ctx_observables", "hx_ctx_read_state", "hx_ctx_write_state",
-    "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_dense_product", "hx_ctx_check_finite", "hx_rhs_noalloc",
+    "hx_ctx_state_device_ptr", "hx_ctx_rhs", "hx_ctx_dense_product", "hx_ctx_inject_wait_timeout", "hx_ctx_check_finite", "hx_rhs_noalloc",
     "hx_ctx_save_snapshot", "hx_ctx_load_snapshot", "hx_write_energy_trace",
     "hx_batch_create", "hx_batch_destroy", "hx_batch_set_stream", "hx_batch_info", "hx_batch_tune",
     "hx_batch_step", "hx_batch_sync", "hx_batch_read_rho0",
@@ -149,6 +149,7 @@ def lib():
             L.hx_ctx_observables.argtypes = [vp, dp, dp, dp]
             L.hx_ctx_read_state.argtypes = [vp, vp, u64]
             L.hx_ctx_dense_product.argtypes = [vp, u32]
+            L.hx_ctx_inject_wait_timeout.argtypes = [vp]
             L.hx_ctx_write_state.argtypes = [vp, vp, u64]
             L.hx_ctx_state_device_ptr.argtypes = [vp, C.POINTER(vp)]
             L.hx_ctx_rhs.argtypes = [vp, vp, u64]
@@ -421,6 +422,10 @@ class Context:
     def dense_product(self, count: int = 1) -> None:
         """Enqueue ``count`` tensor-core products Y = X H_off of a ``dense_h`` context (timing hook)."""
         _check(lib().hx_ctx_dense_product(self._h, C.c_uint32(count)))
+
+    def inject_wait_timeout(self) -> None:
+        """Make the next step's grid-barrier wait run out (failure-detection test hook)."""
+        _check(lib().hx_ctx_inject_wait_timeout(self._h))
 
     def rhs(self) -> np.ndarray:
         out = np.zeros((self.size, self.dim, self.dim), np.complex128)

@@ -327,7 +327,14 @@ int enqueue_step(hx_ctx* c)
     const int m = c->order;
     int launched = 0;
     if (c->use_small_step && !c->closure) {
-        if (hx::launch_small_step(hx::fused_args_of(c), c->rho, c->ua, c->ub, c->dt, m, c->gbar, c->stream, false) != 1)
+        hx::StepWait w;
+        if (c->stall_next_step) {  // test hook: one arrival more than the CTAs make, a short wait
+            w.skew = 1;
+            w.max_polls = 1u << 12;
+            c->stall_next_step = false;
+        }
+        if (hx::launch_small_step(hx::fused_args_of(c), c->rho, c->ua, c->ub, c->dt, m, c->gbar, c->stream, false,
+                                  w) != 1)
             c->launch_failed = true;
         c->counters.kernel_launches += 1;
         c->counters.stage_launches += m;
@@ -1545,6 +1552,15 @@ int hx_ctx_state_device_ptr(hx_ctx* c, void** ptr)
 {
     if (!c || !ptr) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL argument");
     *ptr = c->rho;
+    return HX_OK;
+}
+
+int hx_ctx_inject_wait_timeout(hx_ctx* c)
+{
+    if (!c) return fail(HX_ERR_INVALID_RUNTIME_OPTION, "NULL context");
+    if (!c->use_small_step || c->closure)
+        return fail(HX_ERR_UNSUPPORTED_EXECUTION, "no grid-barrier waits in this context's steps");
+    c->stall_next_step = true;
     return HX_OK;
 }
 

@@ -195,8 +195,14 @@ bool small_supported(int logd, int M, int pauli);
 // launched (with dry: when it would launch), 0 when the ADOs do not fit the resident CTAs (up to 4 per
 // CTA), -1 when refused.
 size_t small_step_smem(int logd, int M, int per);
+// Grid-barrier waits of small_step_kernel: polls before giving up (and setting the error word), and an
+// offset added to every barrier's arrival target (nonzero only to make the waits run out on purpose).
+struct StepWait {
+    unsigned skew = 0;
+    unsigned max_polls = 1u << 24;
+};
 int launch_small_step(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                      unsigned* gcount, cudaStream_t s, bool dry);
+                      unsigned* gcount, cudaStream_t s, bool dry, StepWait w = StepWait{});
 bool launch_small(const FusedArgs& a, const double2* u, const double2* rho, double2* out, double alpha,
                   int base_kind, cudaStream_t s);
 bool prepare_fused(int logd, int M, int J, int herm);  // raises the shared-memory limit; call before stream capture
@@ -413,6 +419,7 @@ struct hx_ctx {
     bool use_small = false;       // d <= 16 sigma_z stage kernel (hx_small.cu)
     bool use_small_step = false;  // ... as one cooperative launch per step (small_step_kernel)
     unsigned* gbar = nullptr;     // grid-barrier arrival counter of small_step_kernel
+    bool stall_next_step = false; // hx_ctx_inject_wait_timeout: the next step's barriers cannot complete
     int sm_count = 0;
     int up_slots = 0;             // ADOs in tier L-1
     int32_t* up_slot = nullptr;   // [H]

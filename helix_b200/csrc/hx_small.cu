@@ -139,7 +139,7 @@ void launch_small_t(const FusedArgs& a, const double2* u, const double2* rho, do
 // every CTA arrives once more and the last to do so puts the counter back to
 // zero, so no host-side count is involved (a captured launch replays
 // correctly).  Returns false when the wait ran out.
-__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned target)
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned target, unsigned max_polls)
 {
     __shared__ int ok;
     __syncthreads();
@@ -152,7 +152,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned target)
             unsigned v;
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
             if (static_cast<int>(v - target) >= 0) break;
-            if (++it > (1u << 24)) {
+            if (++it > max_polls) {
                 ok = 0;
                 break;
             }
@@ -179,7 +179,7 @@ constexpr int kStepPer = 4;
 template <int LOGD, int MAXPER>
 __global__ void __launch_bounds__((1 << (2 * LOGD)) < 32 ? 32 : (1 << (2 * LOGD)), MAXPER == 1 ? 4 : 2)
     small_step_kernel(FusedArgs a, double2* rho, double2* ua, double2* ub, double dt, int order, int per,
-                      unsigned* gcount)
+                      unsigned* gcount, StepWait w)
 {
     constexpr int D = 1 << LOGD, D2 = D * D;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__((1 << (2 * LOGD)) < 32 ? 32 : (1 << (2 * LOGD)
             out[nn[j] * D2 + e] = o;
             x[j] = o;
         }
-        if (st < order && !grid_barrier(gcount, static_cast<unsigned>(st) * G)) {
+        if (st < order && !grid_barrier(gcount, static_cast<unsigned>(st) * G + w.skew, w.max_polls)) {
             if (tid == 0) atomicExch(a.error_flag, 1);
             return;
         }
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__((1 << (2 * LOGD)) < 32 ? 32 : (1 << (2 * LOGD)
 
 template <int LOGD, int MAXPER>
 int launch_small_step_v(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                        unsigned* gcount, cudaStream_t s, bool dry)
+                        unsigned* gcount, cudaStream_t s, bool dry, StepWait w)
 {
     // 1 launched (or would launch, dry), 0 the ADOs do not fit (try the next form), -1 refused
     constexpr int D2 = 1 << (2 * LOGD);
@@ -327,7 +327,8 @@ int launch_small_step_v(const FusedArgs& a, double2* rho, double2* ua, double2* 
         if (dry) return 1;
         FusedArgs args = a;
         int per_arg = per;
-        void* params[] = {&args, &rho, &ua, &ub, &dt, &order, &per_arg, &gcount};
+        StepWait wait = w;
+        void* params[] = {&args, &rho, &ua, &ub, &dt, &order, &per_arg, &gcount, &wait};
         return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(small_step_kernel<LOGD, MAXPER>),
                                            dim3(static_cast<unsigned>(grid)), dim3(threads), params, smem,
                                            s) == cudaSuccess
@@ -339,11 +340,11 @@ int launch_small_step_v(const FusedArgs& a, double2* rho, double2* ua, double2* 
 
 template <int LOGD>
 int launch_small_step_t(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                        unsigned* gcount, cudaStream_t s, bool dry)
+                        unsigned* gcount, cudaStream_t s, bool dry, StepWait w)
 {
-    const int r1 = launch_small_step_v<LOGD, 1>(a, rho, ua, ub, dt, order, gcount, s, dry);
+    const int r1 = launch_small_step_v<LOGD, 1>(a, rho, ua, ub, dt, order, gcount, s, dry, w);
     if (r1 != 0) return r1;
-    return launch_small_step_v<LOGD, kStepPer>(a, rho, ua, ub, dt, order, gcount, s, dry);
+    return launch_small_step_v<LOGD, kStepPer>(a, rho, ua, ub, dt, order, gcount, s, dry, w);
 }
 
 }  // namespace
@@ -363,14 +364,14 @@ size_t small_step_smem(int logd, int M, int per)
 }
 
 int launch_small_step(const FusedArgs& a, double2* rho, double2* ua, double2* ub, double dt, int order,
-                      unsigned* gcount, cudaStream_t s, bool dry)
+                      unsigned* gcount, cudaStream_t s, bool dry, StepWait w)
 {
     if (order < 2) return 0;  // order 1 writes rho while neighbours read it
     switch (a.logd) {
-    case 1: return launch_small_step_t<1>(a, rho, ua, ub, dt, order, gcount, s, dry);
-    case 2: return launch_small_step_t<2>(a, rho, ua, ub, dt, order, gcount, s, dry);
-    case 3: return launch_small_step_t<3>(a, rho, ua, ub, dt, order, gcount, s, dry);
-    case 4: return launch_small_step_t<4>(a, rho, ua, ub, dt, order, gcount, s, dry);
+    case 1: return launch_small_step_t<1>(a, rho, ua, ub, dt, order, gcount, s, dry, w);
+    case 2: return launch_small_step_t<2>(a, rho, ua, ub, dt, order, gcount, s, dry, w);
+    case 3: return launch_small_step_t<3>(a, rho, ua, ub, dt, order, gcount, s, dry, w);
+    case 4: return launch_small_step_t<4>(a, rho, ua, ub, dt, order, gcount, s, dry, w);
     default: return 0;
     }
 }

@@ -283,6 +283,16 @@ int hx_ctx_rhs(hx_ctx* ctx, double* out, uint64_t n);
  * reference. */
 int hx_ctx_dense_product(hx_ctx* ctx, uint32_t count);
 
+/* Failure-detection test hook: the next step of a context whose steps run as
+ * one cooperative launch (small slabs) waits at its first grid barrier for an
+ * arrival that never comes, with a short poll limit.  The kernel gives up,
+ * sets the device error word and returns before writing rho; the next
+ * hx_ctx_sync reports HX_ERR_DEVICE_TIMEOUT, clears the error and the barrier
+ * counter, and the context steps on from the state before the failed step.
+ * HX_ERR_UNSUPPORTED_EXECUTION for other contexts.  No counterpart in the
+ * reference. */
+int hx_ctx_inject_wait_timeout(hx_ctx* ctx);
+
 /* Device check that the state holds only finite values; returns
  * HX_ERR_NON_FINITE otherwise. */
 int hx_ctx_check_finite(hx_ctx* ctx);

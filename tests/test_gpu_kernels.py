@@ -102,3 +102,32 @@ def test_small_step_kernel_replays_from_a_captured_graph(monkeypatch):
         got = ctx.state()
         del graph
     assert np.array_equal(got, want)
+
+
+def test_step_kernel_wait_timeout_is_reported_and_the_context_recovers(monkeypatch):
+    """Failure detection without a GPU fault: the injected step waits at its
+    first grid barrier for an arrival that never comes, gives up after a short
+    poll limit and reports DeviceWaitTimeout; rho is untouched, so the context
+    then steps on exactly as one that never failed."""
+    monkeypatch.setenv("HX_SMALL_STAGE", "1")
+    monkeypatch.setenv("HX_SMALL_STEP", "1")
+    p = S.spin_glass(4, seed=2024, depth=3, K=2, h=1.0, dt=0.01)
+    with capi.Context(p) as ref:
+        ref.step(5)
+        want = ref.state()
+    with capi.Context(p) as ctx:
+        before = ctx.state()
+        ctx.inject_wait_timeout()
+        ctx.step(1)
+        with pytest.raises(capi.HxError) as e:
+            ctx.sync()
+        assert e.value.status == "DeviceWaitTimeout"
+        assert np.array_equal(ctx.state(), before)
+        ctx.step(5)
+        ctx.sync()
+        assert np.array_equal(ctx.state(), want)
+    monkeypatch.setenv("HX_SMALL_STEP", "0")
+    with capi.Context(p) as plain:  # one launch per stage: no grid-barrier waits to run out
+        with pytest.raises(capi.HxError) as e:
+            plain.inject_wait_timeout()
+        assert e.value.status == "UnsupportedExecution"
